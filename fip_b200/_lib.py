@@ -1,0 +1,116 @@
+"""ctypes binding of libfip_b200.so (the C ABI in include/fip.h).
+
+The shared library is built in-tree (fip_b200/libfip_b200.so) by ``make -C fip_b200/csrc`` or
+``__graft_entry__.build()``. There is no fallback: importing the binding without the library
+raises, and every simulation call runs the sm_100a kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfip_b200.so")
+
+FIP_OK = 0
+FIP_ERR_CONFIG = -1
+FIP_ERR_IO = -2
+FIP_ERR_CUDA = -3
+FIP_ERR_NVRTC = -4
+FIP_ERR_NONFINITE = -5
+FIP_ERR_DEVICE_TIMEOUT = -6
+FIP_ERR_ARG = -7
+
+FIELDS = {"h": 0, "qx": 1, "qy": 2, "hmax": 3, "h_prev": 4, "qx_prev": 5, "qy_prev": 6, "terrain": 7, "z": 8}
+
+# every symbol include/fip.h declares
+EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_run", "fip_save", "fip_save_current",
+           "fip_sample", "fip_volume", "fip_get_field", "fip_time", "fip_info", "fip_profile_steps", "fip_destroy",
+           "fip_last_error", "fip_validate", "fip_config_json", "fip_bc_program")
+
+
+class FipOptions(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("use_graphs", ctypes.c_int), ("all_tiles", ctypes.c_int),
+                ("stop_on_nonfinite", ctypes.c_int), ("quiet", ctypes.c_int), ("sample_path", ctypes.c_char_p)]
+
+
+class FipInfo(ctypes.Structure):
+    _fields_ = [("W", ctypes.c_int), ("H", ctypes.c_int), ("pitch", ctypes.c_int), ("n_tiles", ctypes.c_int),
+                ("active_tiles", ctypes.c_int), ("iteration", ctypes.c_int), ("duration", ctypes.c_double),
+                ("dt", ctypes.c_float), ("last_cfl", ctypes.c_float), ("nonfinite", ctypes.c_int)]
+
+
+class FipError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"fip error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C fip_b200/csrc` "
+                              "(or __graft_entry__.build()); there is no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip = ctypes.c_void_p, ctypes.c_int
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.fip_default_options.argtypes = [ctypes.POINTER(FipOptions)]
+        L.fip_default_options.restype = None
+        L.fip_init.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp)]
+        L.fip_init_ex.argtypes = [ctypes.c_char_p, ctypes.POINTER(FipOptions), ctypes.POINTER(vp)]
+        L.fip_step.argtypes = [vp, ip]
+        L.fip_run.argtypes = [vp]
+        L.fip_save.argtypes = [vp, ctypes.c_char_p]
+        L.fip_save_current.argtypes = [vp, ctypes.c_char_p]
+        L.fip_sample.argtypes = [vp]
+        L.fip_volume.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.fip_get_field.argtypes = [vp, ip, fp]
+        L.fip_time.argtypes = [vp, ctypes.POINTER(ctypes.c_double), fp, ctypes.POINTER(ctypes.c_int)]
+        L.fip_info.argtypes = [vp, ctypes.POINTER(FipInfo)]
+        L.fip_profile_steps.argtypes = [vp, ip, fp, fp]
+        L.fip_destroy.argtypes = [vp]
+        L.fip_destroy.restype = None
+        L.fip_last_error.restype = ctypes.c_char_p
+        L.fip_validate.argtypes = [ctypes.c_char_p]
+        L.fip_config_json.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ip]
+        L.fip_bc_program.argtypes = [ctypes.c_char_p, ip, ip, ctypes.c_char_p, ip]
+        for name in ("fip_init", "fip_init_ex", "fip_step", "fip_run", "fip_save", "fip_save_current", "fip_sample",
+                     "fip_volume", "fip_get_field", "fip_time", "fip_info", "fip_profile_steps", "fip_validate",
+                     "fip_config_json", "fip_bc_program"):
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().fip_last_error().decode(errors="replace")
+
+
+def check(rc: int) -> int:
+    if rc < 0:
+        raise FipError(rc, last_error())
+    return rc
+
+
+def validate(yaml_path: str) -> None:
+    check(lib().fip_validate(yaml_path.encode()))
+
+
+def config_json(yaml_path: str) -> dict:
+    import json
+
+    n = check(lib().fip_config_json(yaml_path.encode(), None, 0))
+    buf = ctypes.create_string_buffer(n + 1)
+    check(lib().fip_config_json(yaml_path.encode(), buf, n + 1))
+    return json.loads(buf.value.decode())
+
+
+def bc_program(yaml_path: str, pitch: int, compile: bool = False) -> str:
+    n = check(lib().fip_bc_program(yaml_path.encode(), pitch, int(compile), None, 0))
+    buf = ctypes.create_string_buffer(n + 1)
+    check(lib().fip_bc_program(yaml_path.encode(), pitch, 0, buf, n + 1))
+    return buf.value.decode()

@@ -1,0 +1,400 @@
+#include "bc_codegen.h"
+
+#include <nvrtc.h>
+
+#include "drv.h"
+
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+
+namespace fip {
+
+namespace {
+
+const char kCtlHeader[] =
+#include "fip_ctl_str.inc"
+    ;
+
+// Static part of the program: time-series interpolation and the boundary discharge sum in IEEE
+// float with the host's operation order (the reference evaluates both on the host,
+// src/timeseries.cpp:14-26 and src/boundary_condition.cpp:6-18), the active-tile planner and
+// the control-block advance (controlTimestep, src/main.cpp:25-43).
+const char kPostLib[] = R"FIPSRC(
+#define FIP_G 9.81f
+
+__device__ __forceinline__ float fip_interp(const float* tv, int n, float time) {
+  int lo = 0, hi = n;  // lower_bound: first time not less than `time`
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (tv[mid] < time) lo = mid + 1; else hi = mid;
+  }
+  if (lo == 0) return tv[n];
+  if (lo == n) return tv[2 * n - 1];
+  const float dt = __fsub_rn(tv[lo], tv[lo - 1]);
+  const float f = __fdiv_rn(__fsub_rn(time, tv[lo - 1]), dt);
+  return __fadd_rn(__fmul_rn(f, tv[n + lo]), __fmul_rn(__fsub_rn(1.f, f), tv[n + lo - 1]));
+}
+
+// sequential float sum of sqrt(g a) a over the condition's cells [from, to), a = z - terrain
+// (0 below 1 cm), times dx. Terms are evaluated in parallel, summed in order by thread 0.
+__device__ float fip_sum_depths(const float* sohle, long long base, long long inc, int from, int to, float z,
+                                float dx, float* s_buf) {
+  float acc = 0.f;
+  for (int c0 = from; c0 < to; c0 += 4096) {
+    const int cn = min(4096, to - c0);
+    for (int i = threadIdx.x; i < cn; i += blockDim.x) {
+      float ah = __fsub_rn(z, sohle[base + (long long)(c0 + i) * inc]);
+      if (ah < 0.01f) ah = 0.f;
+      s_buf[i] = __fmul_rn(__fsqrt_rn(__fmul_rn(FIP_G, ah)), ah);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < cn; ++i) acc = __fadd_rn(acc, s_buf[i]);
+    __syncthreads();
+  }
+  return __fmul_rn(acc, dx);
+}
+
+// Active tiles of the next step: a tile is computed when a tile of its 3x3 neighbourhood had a
+// nonzero cell after this step (the stencil reaches 2 cells, less than a tile), when it had one
+// after the previous step (its cells in the output buffer are then not yet equal to the input),
+// or when it is sticky. The flags of the previous step are cleared for reuse.
+__device__ void fip_plan(const FipPostArgs& a, const FipCtl* ctl, int k, int chunk) {
+  __shared__ int s_act[FIP_POST_THREADS / 32];
+  __shared__ int s_inact[FIP_POST_THREADS / 32];
+  const int t = chunk * FIP_PLAN_CHUNK + threadIdx.x;
+  const unsigned char* nzc = a.nz[k & 1];
+  unsigned char* nzp = a.nz[(k + 1) & 1];
+  const bool valid = t < a.n_tiles;
+  bool act = false;
+  if (valid) {
+    const int sx = t / a.n_ty, ty = t - sx * a.n_ty;
+    act = a.sticky[t] || nzp[t] || ctl->force_all;
+    for (int ds = -1; ds <= 1 && !act; ++ds) {
+      const int s2 = sx + ds;
+      if (s2 < 0 || s2 >= a.n_sx) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y2 = ty + dy;
+        if (y2 < 0 || y2 >= a.n_ty) continue;
+        if (nzc[s2 * a.n_ty + y2]) { act = true; break; }
+      }
+    }
+    nzp[t] = 0;
+  }
+  const unsigned ba = __ballot_sync(0xffffffffu, valid && act);
+  const unsigned bi = __ballot_sync(0xffffffffu, valid && !act);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { s_act[warp] = __popc(ba); s_inact[warp] = __popc(bi); }
+  __syncthreads();
+  int base = 0, ibase = 0, total = 0;
+  for (int w = 0; w < FIP_POST_THREADS / 32; ++w) {
+    if (w < warp) { base += s_act[w]; ibase += s_inact[w]; }
+    total += s_act[w];
+  }
+  int* list = a.list[(k + 1) & 1] + chunk * FIP_PLAN_CHUNK;
+  const unsigned below = (1u << lane) - 1u;
+  if (valid && act) list[base + __popc(ba & below)] = t;
+  if (valid && !act) list[FIP_PLAN_CHUNK - 1 - (ibase + __popc(bi & below))] = t;
+  if (threadIdx.x == 0) a.chunk_cnt[(k + 1) & 1][chunk] = total;
+}
+
+// duration += dt (double += float), iteration++, buffer swap, controlTimestep for the next
+// step from this step's CFL minimum, and the checks that end a batch of steps.
+__device__ void fip_advance(FipCtl* ctl) {
+  const int k = ctl->iteration;
+  const float dt = ctl->dt;
+  const float cfl = __uint_as_float(ctl->cfl_bits[k & 1]);
+  ctl->cfl_bits[k & 1] = __float_as_uint(1.0f);
+  ctl->last_cfl = cfl;
+  const double dur = ctl->duration + (double)dt;
+  ctl->duration = dur;
+  ctl->iteration = k + 1;
+  ctl->parity ^= 1;
+  if (ctl->variable_dt) {
+    float min_cfl = 42.0f;
+    if (cfl < min_cfl) min_cfl = cfl;
+    const float target = min_cfl * .5f;
+    const float dc = 0.001f;
+    float d = dt;
+    if (d < target && target - d > dc) d *= 1.001f;
+    else if (d > target && d - target > dc) d *= 0.99f;
+    ctl->dt = d;
+  }
+  int reason = 0;
+  if (--ctl->steps_left <= 0) reason |= FIP_STOP_BUDGET;
+  if (dur >= ctl->next_save) reason |= FIP_STOP_SAVE;
+  if (dur >= ctl->target) reason |= FIP_STOP_TARGET;
+  if (dur >= ctl->next_sample) reason |= FIP_STOP_SAMPLE;
+  if (ctl->nonfinite && ctl->stop_on_nonfinite) reason |= FIP_STOP_NONFINITE;
+  if (ctl->error) reason |= FIP_STOP_ERROR;
+  ctl->post_done = 0u;
+  if (reason) {
+    ctl->stop_reason = reason;
+    __threadfence();
+    ctl->stop = 1;
+  }
+}
+)FIPSRC";
+
+const char kPostKernelHead[] = R"FIPSRC(
+extern "C" __global__ void __launch_bounds__(FIP_POST_THREADS) fip_post(const FipPostArgs a) {
+  __shared__ float s_buf[4096];
+  __shared__ float s_val[2];
+  FipCtl* ctl = a.ctl;
+  if (*((volatile int*)&ctl->stop)) return;
+  const bool step_mode = (a.mode == FIP_POST_MODE_STEP);
+  const int k = step_mode ? ctl->iteration : -1;
+  if (blockIdx.x == 0) {
+    const int cur = step_mode ? (ctl->parity ^ 1) : ctl->parity;
+    const double t_d = step_mode ? ctl->duration + (double)ctl->dt : ctl->duration;
+    const float t = __double2float_rn(t_d);  // TimeSeries::interp(float time)
+    float* h = a.h[cur];
+    float* qx = a.qx[cur];
+    float* qy = a.qy[cur];
+    const float* sohle = a.sohle;
+    const long long W = a.W, H = a.H, pitch = a.pitch;
+    (void)t; (void)W; (void)H; (void)pitch; (void)h; (void)qx; (void)qy; (void)sohle; (void)s_buf; (void)s_val;
+)FIPSRC";
+
+const char kPostKernelTail[] = R"FIPSRC(
+  } else {
+    fip_plan(a, ctl, k, blockIdx.x - 1);
+  }
+  if (!step_mode) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(&ctl->post_done, 1u);
+    if (prev == gridDim.x - 1) {
+      __threadfence();
+      fip_advance(ctl);
+    }
+  }
+}
+)FIPSRC";
+
+std::string flit(float v) {  // exact float literal
+  uint32_t b;
+  std::memcpy(&b, &v, 4);
+  char buf[48];
+  std::snprintf(buf, sizeof buf, "__int_as_float(0x%08x)", b);
+  return buf;
+}
+
+const char* side_name(BcSide s) {
+  switch (s) {
+    case BcSide::left: return "left";
+    case BcSide::right: return "right";
+    case BcSide::top: return "top";
+    default: return "bottom";
+  }
+}
+const char* type_name(BcType t) {
+  switch (t) {
+    case BcType::z: return "z";
+    case BcType::q: return "q";
+    case BcType::close: return "close";
+    default: return "open";
+  }
+}
+
+// src_side_* (src/bc_kernel_gen.cpp:11-73): cell, staggered face and inner neighbour
+void emit_side(std::ostream& o, BcSide side) {
+  switch (side) {
+    case BcSide::right:
+      o << "      const long long idx = tid * pitch + W - 1;\n"
+           "      const long long idx_staggered = idx - 1;\n"
+           "      const long long idx_neighbor = idx - 1;\n"
+           "      float* q = qx;\n      float* q_lateral = qy;\n";
+      break;
+    case BcSide::left:
+      o << "      const long long idx = tid * pitch;\n"
+           "      const long long idx_staggered = idx;\n"
+           "      const long long idx_neighbor = idx + 1;\n"
+           "      float* q = qx;\n      float* q_lateral = qy;\n";
+      break;
+    case BcSide::top:
+      o << "      const long long idx = tid + (H - 1) * pitch;\n"
+           "      const long long idx_staggered = idx - pitch;\n"
+           "      const long long idx_neighbor = idx - pitch;\n"
+           "      float* q = qy;\n      float* q_lateral = qx;\n";
+      break;
+    case BcSide::bottom:
+      o << "      const long long idx = tid;\n"
+           "      const long long idx_staggered = idx;\n"
+           "      const long long idx_neighbor = idx + pitch;\n"
+           "      float* q = qy;\n      float* q_lateral = qx;\n";
+      break;
+  }
+  o << "      (void)idx_staggered; (void)q_lateral;\n";
+}
+
+// src_type_* (src/bc_kernel_gen.cpp:75-137); `staggered` for the rmg solver
+void emit_type(std::ostream& o, BcType type, bool staggered) {
+  const char* qi = staggered ? "idx_staggered" : "idx";
+  switch (type) {
+    case BcType::z:
+      if (staggered)
+        o << "      h[idx] = fmaxf(0.f, zval - sohle[idx]);\n"
+             "      h[idx_neighbor] = fmaxf(0.f, zval - sohle[idx_neighbor]);\n"
+             "      q[idx_staggered] = -0.f;\n";
+      else
+        o << "      const float ah = fmaxf(0.f, zval - sohle[idx]);\n"
+             "      h[idx] = ah;\n"
+             "      q[idx] = 0.99f * (q[idx_neighbor] / fmaxf(h[idx_neighbor], 0.01f)) * ah;\n";
+      break;
+    case BcType::q:
+      o << "      float ah = zval - sohle[idx];\n"
+           "      if (ah < 0.f) ah = 0.f;\n"
+           "      q["
+        << qi << "] = sqrtf(FIP_G * ah) * ah * qval;\n";
+      if (staggered)
+        o << "      if (ah > 0.f) {\n"
+             "        const float z_neighbor = h[idx_neighbor] + sohle[idx_neighbor];\n"
+             "        h[idx] = fmaxf(ah / 2, z_neighbor - sohle[idx]);\n"
+             "      }\n";
+      else
+        o << "      if (ah > 0.f) h[idx] = fmaxf(ah / 2, h[idx_neighbor] + sohle[idx_neighbor] - sohle[idx]);\n";
+      break;
+    case BcType::close:
+      o << "      q[" << qi
+        << "] = 0.f;\n"
+           "      q_lateral[idx] = q_lateral[idx_neighbor];\n"
+           "      h[idx] = h[idx_neighbor];\n";
+      break;
+    case BcType::open:
+      o << "      const float ah_neighbor = h[idx_neighbor];\n"
+           "      const float z_neighbor = ah_neighbor + sohle[idx_neighbor];\n"
+           "      const float sign = (float)(idx - idx_neighbor);\n"
+           "      if (ah_neighbor > 0.f) {\n"
+           "        q["
+        << qi
+        << "] = sign * sqrtf(FIP_G * ah_neighbor) * ah_neighbor;\n"
+           "        h[idx] = fminf(ah_neighbor, fmaxf(0.f, z_neighbor - sohle[idx]));\n"
+           "      }\n";
+      break;
+  }
+}
+
+}  // namespace
+
+SeriesLayout layout_series(const Config& cfg) {
+  SeriesLayout s;
+  for (const BoundaryCondition& bc : cfg.bcs) {
+    auto put = [&](const TimeSeries& ts, bool has, std::vector<long>& off, std::vector<int>& n) {
+      if (!bc.is_series || !has) {
+        off.push_back(-1);
+        n.push_back(0);
+        return;
+      }
+      off.push_back((long)s.data.size());
+      n.push_back((int)ts.t.size());
+      s.data.insert(s.data.end(), ts.t.begin(), ts.t.end());
+      s.data.insert(s.data.end(), ts.v.begin(), ts.v.end());
+    };
+    put(bc.z_series, bc.has_z_series, s.z_off, s.z_n);
+    put(bc.q_series, bc.has_q_series, s.q_off, s.q_n);
+  }
+  if (s.data.empty()) s.data.push_back(0.f);
+  return s;
+}
+
+std::string post_kernel_source(const Config& cfg, const SeriesLayout& ser, int pitch) {
+  std::ostringstream o;
+  o << "// generated by fip_b200 from " << cfg.yaml_path << "\n";
+  o << kCtlHeader << kPostLib << kPostKernelHead;
+  for (size_t i = 0; i < cfg.bcs.size(); ++i) {
+    const BoundaryCondition& bc = cfg.bcs[i];
+    o << "    {  // condition " << i << ": " << side_name(bc.side) << " " << type_name(bc.type) << ", cells "
+      << bc.from << ".." << bc.to << (bc.is_series ? ", time series" : "") << "\n";
+    if (!bc.is_series) {
+      o << "      const float zval = " << flit(cfg.const_z(bc)) << ";\n";
+      o << "      const float qval = " << flit(cfg.const_q(bc)) << ";\n";
+    } else {
+      // getZ / getQ of BoundaryConditionTimeseries (src/boundary_condition.cpp:56-77)
+      o << "      if (threadIdx.x == 0) s_val[0] = ";
+      if (ser.z_off[i] >= 0)
+        o << "fip_interp(a.series + " << ser.z_off[i] << "L, " << ser.z_n[i] << ", t);\n";
+      else
+        o << "0.f;\n";
+      o << "      __syncthreads();\n      const float zval = s_val[0];\n";
+      if (bc.type == BcType::q) {
+        long long base = 0, inc = 1;
+        switch (bc.side) {
+          case BcSide::left: base = 0; inc = pitch; break;
+          case BcSide::right: base = (long long)cfg.W - 1; inc = pitch; break;
+          case BcSide::top: base = (long long)(cfg.H - 1) * pitch; inc = 1; break;
+          case BcSide::bottom: base = 0; inc = 1; break;
+        }
+        o << "      const float wsum = fip_sum_depths(sohle, " << base << "LL, " << inc << "LL, " << bc.from << ", "
+          << bc.to << ", zval, a.dx, s_buf);\n";
+        o << "      if (threadIdx.x == 0) s_val[1] = __fdiv_rn(fip_interp(a.series + " << ser.q_off[i] << "L, "
+          << ser.q_n[i] << ", t), wsum);\n";
+        o << "      __syncthreads();\n      const float qval = s_val[1];\n";
+      } else {
+        o << "      const float qval = 0.f;\n";
+      }
+    }
+    o << "      (void)zval; (void)qval;\n";
+    o << "      for (long long tid = " << bc.from << " + (long long)threadIdx.x; tid <= " << bc.to
+      << "; tid += blockDim.x) {\n";
+    emit_side(o, bc.side);
+    emit_type(o, bc.type, cfg.staggered());
+    o << "      }\n      __syncthreads();\n    }\n";
+  }
+  o << kPostKernelTail;
+  return o.str();
+}
+
+int compile_post_kernel(const std::string& source, std::string* cubin, std::string* log, std::string* err) {
+  nvrtcProgram prog;
+  nvrtcResult r = nvrtcCreateProgram(&prog, source.c_str(), "fip_post.cu", 0, nullptr, nullptr);
+  if (r != NVRTC_SUCCESS) {
+    *err = std::string("nvrtcCreateProgram: ") + nvrtcGetErrorString(r);
+    return -1;
+  }
+  const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--diag-suppress=177"};
+  r = nvrtcCompileProgram(prog, 3, opts);
+  size_t log_size = 0;
+  nvrtcGetProgramLogSize(prog, &log_size);
+  log->assign(log_size, '\0');
+  if (log_size) nvrtcGetProgramLog(prog, &(*log)[0]);
+  if (r != NVRTC_SUCCESS) {
+    *err = std::string("NVRTC compile of the boundary-condition kernel failed: ") + nvrtcGetErrorString(r) + "\n" + *log;
+    nvrtcDestroyProgram(&prog);
+    return -1;
+  }
+  size_t n = 0;
+  nvrtcGetCUBINSize(prog, &n);
+  cubin->assign(n, '\0');
+  nvrtcGetCUBIN(prog, &(*cubin)[0]);
+  nvrtcDestroyProgram(&prog);
+  return 0;
+}
+
+int build_post_kernel(const std::string& source, PostKernel* out, std::string* err) {
+  std::string cubin;
+  out->source = source;
+  if (compile_post_kernel(source, &cubin, &out->log, err)) return -1;
+  if (!drv::load(err)) return -1;
+  CUresult cr = drv::ModuleLoadData(&out->module, cubin.data());
+  if (cr != CUDA_SUCCESS) {
+    *err = drv::message(cr, "cuModuleLoadData");
+    return -1;
+  }
+  cr = drv::ModuleGetFunction(&out->fn, out->module, "fip_post");
+  if (cr != CUDA_SUCCESS) {
+    *err = "cuModuleGetFunction(fip_post) failed";
+    return -1;
+  }
+  return 0;
+}
+
+void destroy_post_kernel(PostKernel* k) {
+  if (k->module && drv::ModuleUnload) drv::ModuleUnload(k->module);
+  k->module = nullptr;
+  k->fn = nullptr;
+}
+
+}  // namespace fip

@@ -1,0 +1,43 @@
+// Boundary-condition kernel generation (the reference's BoundaryConditionKernel, src/bc_kernel_gen.{h,cpp}).
+// The YAML's conditions become one CUDA program, compiled at start-up with NVRTC straight to an
+// sm_100a cubin and loaded with the driver API. The program's single kernel, fip_post, runs after
+// every step: block 0 applies the conditions one after the other (configuration order), the
+// other blocks build the next active-tile list, and the last block to finish advances the
+// device control block (time, dt controller, iteration, event checks).
+#pragma once
+#include <cuda.h>
+
+#include <string>
+#include <vector>
+
+#include "config.h"
+#include "fip_ctl.h"
+
+namespace fip {
+
+struct SeriesLayout {
+  std::vector<float> data;      // concatenated tables, uploaded to the device
+  std::vector<long> z_off, q_off;  // per condition: offset of its z / q table (-1: none)
+  std::vector<int> z_n, q_n;
+};
+
+SeriesLayout layout_series(const Config& cfg);
+
+// CUDA source of the post kernel for `cfg` (pitch in elements: the top/bottom open boundary
+// scales its outflow by idx - idx_neighbor = +-pitch, src/bc_kernel_gen.cpp:122, :132).
+std::string post_kernel_source(const Config& cfg, const SeriesLayout& ser, int pitch);
+
+struct PostKernel {
+  CUmodule module = nullptr;
+  CUfunction fn = nullptr;
+  std::string source, log;
+};
+
+// NVRTC compile for sm_100a to a cubin (no GPU needed). Returns 0 or a message in *err.
+int compile_post_kernel(const std::string& source, std::string* cubin, std::string* log, std::string* err);
+
+// compile_post_kernel + cuModuleLoadData. Returns 0 or a message in *err.
+int build_post_kernel(const std::string& source, PostKernel* out, std::string* err);
+void destroy_post_kernel(PostKernel* k);
+
+}  // namespace fip

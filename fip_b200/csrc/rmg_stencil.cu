@@ -1,0 +1,806 @@
+// sm_100a kernels of the slim shallow-water step (fip's rmg solver).
+//
+// rmg_step_kernel restates one launch of the reference's rmg_kernel (src/kernels.cu:264-438)
+// with the wet/dry mask replaced by an exact active-tile list:
+//   * momentum fluxes fx/fy/gx/gy, the semi-implicit Strickler update of qx/qy with the flux
+//     limiter (compute_rmg_qx/qy, src/kernels.cu:75-127), the boundary-face holds (:373-376),
+//     continuity (:381), the three write sets (:383-406) and the CFL fold (:392-400), all in
+//     FP32 with the same expression trees (compiled with -use_fast_math like the reference, so
+//     sqrtf/powf/division are the same approximations);
+//   * the domain is cut into tiles of 480 columns x 32 rows. A CTA has four consumer warps
+//     (each thread owns 4 adjacent columns, a warp 128 columns of which the 120 inner ones are
+//     stored) and one producer warp that streams rows of h/qx/qy/terrain/kSt into an 8-slot
+//     shared-memory ring with TMA (cp.async.bulk.tensor, no multicast). Consumers march north
+//     row by row, keeping the vertical window in registers and exchanging east/west
+//     neighbours with warp shuffles;
+//   * work = the concatenation of the active tiles' rows (strip-major), split evenly over the
+//     persistent CTAs, so vertically adjacent active tiles are marched without re-staging;
+//   * each CTA folds its CFL minimum into ctl->cfl_bits with one atomicMin per warp, marks the
+//     tiles whose new state has a nonzero cell, and (every hmax_every iterations) folds hmax.
+// Every wait on an mbarrier is bounded (2 s of %globaltimer); on expiry the kernel records
+// FIP_DEVERR_* in ctl->error and returns after draining its own copies.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "drv.h"
+#include "fip_ctl.h"
+#include "rmg_stencil.h"
+
+namespace fip {
+
+namespace {
+
+constexpr float kDH = 0.01f;         // src/kernels.cu:23
+constexpr float kEPS = 10e-7f;       // src/kernels.cu:24 (EPS_TROCKEN)
+constexpr float kG = 9.81f;          // src/simdata.h:358
+constexpr int kNSlot = 8;            // ring depth in rows
+constexpr int kFieldBytes = FIP_SMEM_COLS * 4;  // 2048 B per staged row of one field
+constexpr int kConsumerWarps = 4;
+constexpr int kThreads = (kConsumerWarps + 1) * 32;
+constexpr int kMaxChunks = 256;
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+enum { F_H = 0, F_QX = 1, F_QY = 2, F_S = 3, F_K = 4 };
+
+struct StepArgs {
+  float* h[2];
+  float* qx[2];
+  float* qy[2];
+  float* hmax;
+  FipCtl* ctl;
+  const int* list[2];
+  const int* chunk_cnt[2];
+  unsigned char* nz[2];
+  int W, H, pitch;
+  int n_sx, n_ty, n_tiles, n_chunks;
+  float dx, kst_fixed, no_value;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of `parity` to complete; false after kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 0 && globaltimer() - t0 > kWaitNs) return false;
+  }
+}
+__device__ __forceinline__ void tma_row(void* dst, const CUtensorMap* tm, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void record_error(FipCtl* ctl, int code) { atomicCAS(&ctl->error, 0, code); }
+
+// fp32div_wrapper (src/kernels.cu:30-33)
+__device__ __forceinline__ float fdivw(float a, float b) { return (a == 0.0f) ? 0.0f : (a / b); }
+
+// compute_rmg_qx (src/kernels.cu:75-100); same operand order, so the same rounding
+__device__ __forceinline__ float upd_qx(float fx_east, float fx_i, float gx_i, float gx_south, float dt, float dx,
+                                        float dt_inv, float dx_inv, float kst, float h_i, float h_east,
+                                        float s_east, float s_i, float qx_i, float qy_i, float qy_e, float qy_s,
+                                        float qy_se) {
+  float dfx = (fx_east - fx_i) * dx_inv;
+  float dgx = (gx_i - gx_south) * dx_inv;
+  float a = (h_i + h_east) * .5f;
+  a = fmaxf(0.f, a);
+  float dhg = a * kG * (-s_east + s_i) * dx_inv;
+  float dhx = (0.5f * kG * h_east * h_east - 0.5f * kG * h_i * h_i) * dx_inv;
+  a = fmaxf(a, kDH);
+  const float inv = 1.f / a;
+  const float ux = qx_i;
+  const float uy = (qy_i + qy_e + qy_s + qy_se) * 0.25f;
+  float reib = ((ux == 0.f) && (uy == 0.f)) ? 0.f : (dt * kG / (kst * kst) * sqrtf(ux * ux + uy * uy) * powf(inv, 2.33f));
+  float q = fdivw(qx_i + dt * (-dfx - dgx - dhx + dhg), (1.f + reib));
+  q = fminf(q, h_i * dt_inv * dx * 0.25f);
+  q = fmaxf(q, -h_east * dt_inv * dx * 0.25f);
+  return q;
+}
+
+// compute_rmg_qy (src/kernels.cu:102-127)
+__device__ __forceinline__ float upd_qy(float fy_i, float fy_west, float gy_i, float gy_north, float dt, float dx,
+                                        float dt_inv, float dx_inv, float kst, float h_i, float h_north,
+                                        float s_north, float s_i, float qy_i, float qx_i, float qx_w, float qx_n,
+                                        float qx_nw) {
+  float dgy = (gy_north - gy_i) * dx_inv;
+  float dfy = (fy_i - fy_west) * dx_inv;
+  float a = (h_i + h_north) * .5f;
+  a = fmaxf(0.f, a);
+  float dhg = a * kG * (s_i - s_north) * dx_inv;
+  float dhy = (0.5f * kG * h_north * h_north - 0.5f * kG * h_i * h_i) * dx_inv;
+  a = fmaxf(a, kDH);
+  float inv = 1.f / a;
+  float ux = (qx_i + qx_n + qx_w + qx_nw) * 0.25f;
+  float uy = qy_i;
+  float reib = ((ux == 0.f) && (uy == 0.f)) ? 0.f : (dt * kG / (kst * kst) * sqrtf(ux * ux + uy * uy) * powf(inv, 2.33f));
+  float q = fdivw(qy_i + dt * (-dgy - dfy - dhy + dhg), (1 + reib));
+  q = fminf(q, h_i * dt_inv * dx * 0.25f);
+  q = fmaxf(q, -h_north * dt_inv * dx * 0.25f);
+  return q;
+}
+
+__device__ __forceinline__ float4 lds4(const unsigned char* slot, int field, int col) {
+  return *reinterpret_cast<const float4*>(slot + field * kFieldBytes + col * 4);
+}
+
+// Walk of a CTA's share of the active-tile row stream: maximal runs of rows that are
+// contiguous in one strip (vertically adjacent active tiles are one run).
+struct Walk {
+  long long pos, end;
+};
+
+__device__ __forceinline__ int list_entry(const int* list, const int* s_prefix, int n_chunks, long long p) {
+  int c = 0;
+  while (c + 1 < n_chunks && s_prefix[c + 1] <= p) ++c;
+  return list[c * FIP_PLAN_CHUNK + (int)(p - s_prefix[c])];
+}
+
+__device__ __forceinline__ bool next_run(Walk& w, const int* list, const int* s_prefix, int n_chunks, int n_ty, int H,
+                                         int* strip, int* ra, int* rb) {
+  while (w.pos < w.end) {
+    long long p = w.pos / FIP_TILE_ROWS;
+    const int off = (int)(w.pos - p * FIP_TILE_ROWS);
+    int tile = list_entry(list, s_prefix, n_chunks, p);
+    const int s = tile / n_ty;
+    const int ty0 = tile - s * n_ty;
+    int ty = ty0;
+    // extend over the following list entries while they are the next tile up the same strip
+    while ((p + 1) * FIP_TILE_ROWS < w.end && ty + 1 < n_ty &&
+           list_entry(list, s_prefix, n_chunks, p + 1) == tile + 1) {
+      ++p;
+      ++tile;
+      ++ty;
+    }
+    const long long stop = (p + 1) * FIP_TILE_ROWS < w.end ? (p + 1) * FIP_TILE_ROWS : w.end;
+    const int r_a = ty0 * FIP_TILE_ROWS + off;
+    int r_b = ty * FIP_TILE_ROWS + (int)(stop - p * FIP_TILE_ROWS);
+    w.pos = stop;
+    if (r_b > H) r_b = H;
+    if (r_a >= r_b) continue;  // rows entirely beyond the grid
+    *strip = s;
+    *ra = r_a;
+    *rb = r_b;
+    return true;
+  }
+  return false;
+}
+
+template <bool KVAR>
+__global__ void __launch_bounds__(kThreads, 2)
+    rmg_step_kernel(const __grid_constant__ CUtensorMap tm_h0, const __grid_constant__ CUtensorMap tm_h1,
+                    const __grid_constant__ CUtensorMap tm_qx0, const __grid_constant__ CUtensorMap tm_qx1,
+                    const __grid_constant__ CUtensorMap tm_qy0, const __grid_constant__ CUtensorMap tm_qy1,
+                    const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_k,
+                    const StepArgs a) {
+  constexpr int NF = KVAR ? 5 : 4;
+  constexpr int kSlotBytes = NF * kFieldBytes;
+  extern __shared__ __align__(1024) unsigned char smem_dyn[];
+  __shared__ __align__(8) uint64_t full_bar[kNSlot];
+  __shared__ __align__(8) uint64_t empty_bar[kNSlot];
+  __shared__ int s_prefix[kMaxChunks + 1];
+  __shared__ int s_hdr[6];
+
+  unsigned char* ring = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
+  FipCtl* ctl = a.ctl;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    s_hdr[0] = *((volatile int*)&ctl->stop);
+    s_hdr[1] = ctl->parity;
+    s_hdr[2] = ctl->iteration;
+    s_hdr[3] = __float_as_int(ctl->dt);
+    s_hdr[4] = (ctl->hmax_every > 0 && ctl->iteration > 0 && ctl->iteration % ctl->hmax_every == 0) ? 1 : 0;
+    s_hdr[5] = ctl->hmax_full;
+    for (int i = 0; i < kNSlot; ++i) {
+      mbar_init(&full_bar[i], 1);
+      mbar_init(&empty_bar[i], kConsumerWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (tid < 32) {  // prefix over the chunk counts of this step's plan
+    const int par = ctl->parity;
+    const int* cnt = a.chunk_cnt[(ctl->iteration) & 1];
+    (void)par;
+    if (lane == 0) {
+      int acc = 0;
+      for (int c = 0; c < a.n_chunks; ++c) {
+        s_prefix[c] = acc;
+        acc += cnt[c];
+      }
+      s_prefix[a.n_chunks] = acc;
+    }
+  }
+  __syncthreads();
+  if (s_hdr[0]) return;
+
+  const int par = s_hdr[1];
+  const int it = s_hdr[2];
+  const float dt = __int_as_float(s_hdr[3]);
+  const bool fold = s_hdr[4] != 0;
+  const int* list = a.list[it & 1];
+  const long long total = (long long)s_prefix[a.n_chunks] * FIP_TILE_ROWS;
+  const long long G = gridDim.x;
+  Walk walk0;
+  walk0.pos = total * blockIdx.x / G;
+  walk0.end = total * (blockIdx.x + 1) / G;
+
+  if (warp == kConsumerWarps) {
+    // ---------------- producer: one elected thread streams rows with TMA ----------------
+    if (lane == 0) {
+      const CUtensorMap* th = par ? &tm_h1 : &tm_h0;
+      const CUtensorMap* tqx = par ? &tm_qx1 : &tm_qx0;
+      const CUtensorMap* tqy = par ? &tm_qy1 : &tm_qy0;
+      Walk w = walk0;
+      uint32_t seq = 0;
+      bool ok = true;
+      int s, ra, rb;
+      while (ok && next_run(w, list, s_prefix, a.n_chunks, a.n_ty, a.H, &s, &ra, &rb)) {
+        const int x0 = s * FIP_TILE_COLS - FIP_SMEM_X0;
+        for (int j = ra - 2; j <= rb + 1; ++j, ++seq) {
+          const uint32_t slot = seq % kNSlot;
+          const uint32_t ph = (seq / kNSlot) & 1u;
+          if (!mbar_wait(&empty_bar[slot], ph ^ 1u)) {
+            record_error(ctl, FIP_DEVERR_WAIT_EMPTY);
+            ok = false;
+            break;
+          }
+          unsigned char* dst = ring + slot * kSlotBytes;
+          mbar_arrive_expect_tx(&full_bar[slot], kSlotBytes);
+          tma_row(dst + F_H * kFieldBytes, th, x0, j, &full_bar[slot]);
+          tma_row(dst + F_H * kFieldBytes + 1024, th, x0 + 256, j, &full_bar[slot]);
+          tma_row(dst + F_QX * kFieldBytes, tqx, x0, j, &full_bar[slot]);
+          tma_row(dst + F_QX * kFieldBytes + 1024, tqx, x0 + 256, j, &full_bar[slot]);
+          tma_row(dst + F_QY * kFieldBytes, tqy, x0, j, &full_bar[slot]);
+          tma_row(dst + F_QY * kFieldBytes + 1024, tqy, x0 + 256, j, &full_bar[slot]);
+          tma_row(dst + F_S * kFieldBytes, &tm_s, x0, j, &full_bar[slot]);
+          tma_row(dst + F_S * kFieldBytes + 1024, &tm_s, x0 + 256, j, &full_bar[slot]);
+          if (KVAR) {
+            tma_row(dst + F_K * kFieldBytes, &tm_k, x0, j, &full_bar[slot]);
+            tma_row(dst + F_K * kFieldBytes + 1024, &tm_k, x0 + 256, j, &full_bar[slot]);
+          }
+        }
+      }
+      // drain: never leave the CTA with copies in flight into its shared memory
+      const uint32_t n_in_flight = seq < (uint32_t)kNSlot ? seq : (uint32_t)kNSlot;
+      for (uint32_t i = 0; i < n_in_flight; ++i) {
+        const uint32_t q = seq - 1 - i;
+        if (!mbar_wait(&full_bar[q % kNSlot], (q / kNSlot) & 1u)) {
+          record_error(ctl, FIP_DEVERR_WAIT_DRAIN);
+          break;
+        }
+      }
+    }
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  const float dx = a.dx;
+  const float dx_inv = 1.f / dx;  // in-kernel, as the reference (:276-277)
+  const float dt_inv = 1.f / dt;
+  const int W = a.W, H = a.H, pitch = a.pitch;
+  const float nv = a.no_value;
+  const int scol = FIP_SMEM_X0 - 4 + 120 * warp + 4 * lane;  // staged column of k = 0
+  const bool out_lane = (lane >= 1 && lane <= 30);
+  float* const h_out = a.h[par ^ 1];
+  float* const qx_out = a.qx[par ^ 1];
+  float* const qy_out = a.qy[par ^ 1];
+  const float* const h_in = a.h[par];
+  unsigned char* const nzs = a.nz[it & 1];
+
+  float cfl = 1.0f;
+  bool bad = false;
+  uint32_t seq = 0;
+  Walk w = walk0;
+  int s, ra, rb;
+  while (next_run(w, list, s_prefix, a.n_chunks, a.n_ty, H, &s, &ra, &rb)) {
+    const int c = s * FIP_TILE_COLS - 4 + 120 * warp + 4 * lane;  // global column of k = 0
+    bool colH[4], colQX[4], colQY[4], holdX[4], colIn[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int cc = c + k;
+      colH[k] = out_lane && cc >= 1 && cc <= W - 2;
+      colQX[k] = out_lane && cc >= 1 && cc <= W - 3;
+      colQY[k] = out_lane && cc >= 2 && cc <= W - 3;
+      holdX[k] = (cc == 0 || cc == W - 2);
+      colIn[k] = out_lane && cc >= 0 && cc < W;
+    }
+    const uint32_t seq0 = seq;
+    auto slot_of = [&](int row) -> const unsigned char* {
+      return ring + ((seq0 + (uint32_t)(row - (ra - 2))) % kNSlot) * kSlotBytes;
+    };
+    auto wait_row = [&](int row) -> bool {  // warp-uniform: every lane waits, all must succeed
+      const uint32_t q = seq0 + (uint32_t)(row - (ra - 2));
+      const bool got = mbar_wait(&full_bar[q % kNSlot], (q / kNSlot) & 1u);
+      return __all_sync(0xffffffffu, got);
+    };
+    auto release_row = [&](int row) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty_bar[(seq0 + (uint32_t)(row - (ra - 2))) % kNSlot]);
+    };
+
+    bool ok = wait_row(ra - 2) && wait_row(ra - 1) && wait_row(ra);
+    if (!ok) {
+      record_error(ctl, FIP_DEVERR_WAIT_FULL);
+      break;
+    }
+    // ---- prologue: rows ra-2 .. ra ----
+    float h0[4], h1[4], hE0, hE1;
+    float qx0[4], qxW0, qy0[4], qyE0, qyS[4], qySE, s0[4], sE0;
+    float ux0[4], uxW0, uy0[4], uyE0, uyS[4], gxS[4], gy0[4], qy2S[4];
+    {
+      const float4 vhs = lds4(slot_of(ra - 2), F_H, scol);
+      const float4 vqys = lds4(slot_of(ra - 2), F_QY, scol);
+      const float4 vh0 = lds4(slot_of(ra - 1), F_H, scol);
+      const float4 vqx0 = lds4(slot_of(ra - 1), F_QX, scol);
+      const float4 vqy0 = lds4(slot_of(ra - 1), F_QY, scol);
+      const float4 vs0 = lds4(slot_of(ra - 1), F_S, scol);
+      const float4 vh1 = lds4(slot_of(ra), F_H, scol);
+      const float hs[4] = {vhs.x, vhs.y, vhs.z, vhs.w};
+      qyS[0] = vqys.x; qyS[1] = vqys.y; qyS[2] = vqys.z; qyS[3] = vqys.w;
+      h0[0] = vh0.x; h0[1] = vh0.y; h0[2] = vh0.z; h0[3] = vh0.w;
+      qx0[0] = vqx0.x; qx0[1] = vqx0.y; qx0[2] = vqx0.z; qx0[3] = vqx0.w;
+      qy0[0] = vqy0.x; qy0[1] = vqy0.y; qy0[2] = vqy0.z; qy0[3] = vqy0.w;
+      s0[0] = vs0.x; s0[1] = vs0.y; s0[2] = vs0.z; s0[3] = vs0.w;
+      h1[0] = vh1.x; h1[1] = vh1.y; h1[2] = vh1.z; h1[3] = vh1.w;
+      qySE = __shfl_down_sync(0xffffffffu, qyS[0], 1);
+      hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
+      qxW0 = __shfl_up_sync(0xffffffffu, qx0[3], 1);
+      qyE0 = __shfl_down_sync(0xffffffffu, qy0[0], 1);
+      sE0 = __shfl_down_sync(0xffffffffu, s0[0], 1);
+      hE1 = __shfl_down_sync(0xffffffffu, h1[0], 1);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        uyS[k] = fdivw(qyS[k], fmaxf(fmaxf(kDH, hs[k]), h0[k]));
+        ux0[k] = fdivw(qx0[k], fmaxf(fmaxf(kDH, h0[k]), k < 3 ? h0[k + 1] : hE0));
+        uy0[k] = fdivw(qy0[k], fmaxf(fmaxf(kDH, h0[k]), h1[k]));
+      }
+      uxW0 = __shfl_up_sync(0xffffffffu, ux0[3], 1);
+      uyE0 = __shfl_down_sync(0xffffffffu, uy0[0], 1);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        // compute_rmg_gy for row ra-1: uy_i = uy(ra-1), uy_south = uy(ra-2)
+        gy0[k] = (uy0[k] + uyS[k] > 0) ? qyS[k] * uyS[k] : qy0[k] * uy0[k];
+        gxS[k] = 0.f;
+        qy2S[k] = 0.f;
+      }
+    }
+    release_row(ra - 2);
+
+    bool nzf = false;
+    for (int r = ra - 1; r < rb; ++r) {
+      if (!wait_row(r + 2)) {
+        record_error(ctl, FIP_DEVERR_WAIT_FULL);
+        ok = false;
+        break;
+      }
+      const unsigned char* sl0 = slot_of(r);
+      const unsigned char* sl1 = slot_of(r + 1);
+      const unsigned char* sl2 = slot_of(r + 2);
+      float h2r[4], qx1[4], qy1[4], s1[4], kk[4];
+      {
+        const float4 v2 = lds4(sl2, F_H, scol);
+        const float4 vqx = lds4(sl1, F_QX, scol);
+        const float4 vqy = lds4(sl1, F_QY, scol);
+        const float4 vs = lds4(sl1, F_S, scol);
+        h2r[0] = v2.x; h2r[1] = v2.y; h2r[2] = v2.z; h2r[3] = v2.w;
+        qx1[0] = vqx.x; qx1[1] = vqx.y; qx1[2] = vqx.z; qx1[3] = vqx.w;
+        qy1[0] = vqy.x; qy1[1] = vqy.y; qy1[2] = vqy.z; qy1[3] = vqy.w;
+        s1[0] = vs.x; s1[1] = vs.y; s1[2] = vs.z; s1[3] = vs.w;
+        if (KVAR) {
+          const float4 vk = lds4(sl0, F_K, scol);
+          kk[0] = vk.x; kk[1] = vk.y; kk[2] = vk.z; kk[3] = vk.w;
+        } else {
+          kk[0] = kk[1] = kk[2] = kk[3] = a.kst_fixed;
+        }
+      }
+      release_row(r);
+      const float hE2 = __shfl_down_sync(0xffffffffu, h2r[0], 1);
+      const float qxW1 = __shfl_up_sync(0xffffffffu, qx1[3], 1);
+      const float qyE1 = __shfl_down_sync(0xffffffffu, qy1[0], 1);
+      const float sE1 = __shfl_down_sync(0xffffffffu, s1[0], 1);
+
+      // velocities of row r+1 (src/kernels.cu:351-354)
+      float ux1[4], uy1[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        ux1[k] = fdivw(qx1[k], fmaxf(fmaxf(kDH, h1[k]), k < 3 ? h1[k + 1] : hE1));
+        uy1[k] = fdivw(qy1[k], fmaxf(fmaxf(kDH, h1[k]), h2r[k]));
+      }
+      const float ux1W = __shfl_up_sync(0xffffffffu, ux1[3], 1);
+      const float uy1E = __shfl_down_sync(0xffffffffu, uy1[0], 1);
+
+      float fx[4], fy[4], gx[4], gy1[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        // compute_rmg_fy (:45-54): ux at the cell and its north neighbour
+        const float uh = (ux0[k] + ux1[k]) * .5f;
+        fy[k] = (ux0[k] + ux1[k] > 0) ? qy0[k] * uh : (k < 3 ? qy0[k + 1] : qyE0) * uh;
+        // compute_rmg_gy for row r+1 (:65-73, called at :359)
+        gy1[k] = (uy1[k] + uy0[k] > 0) ? qy0[k] * uy0[k] : qy1[k] * uy1[k];
+        // compute_rmg_gx (:35-43)
+        const float ue = k < 3 ? uy0[k + 1] : uyE0;
+        const float vh = (uy0[k] + ue) * .5f;
+        gx[k] = (uy0[k] + ue > 0) ? qx0[k] * vh : qx1[k] * vh;
+        // compute_rmg_fx (:56-63)
+        const float uw = k > 0 ? ux0[k - 1] : uxW0;
+        const float qw = k > 0 ? qx0[k - 1] : qxW0;
+        fx[k] = (uw + ux0[k] > 0) ? qw * uw : qx0[k] * ux0[k];
+      }
+      const float fyW = __shfl_up_sync(0xffffffffu, fy[3], 1);
+      const float fxE = __shfl_down_sync(0xffffffffu, fx[0], 1);
+
+      const bool hold_y = (r == 0 || r == H - 2);
+      float qx2[4], qy2[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float fq = upd_qx(k < 3 ? fx[k + 1] : fxE, fx[k], gx[k], gxS[k], dt, dx, dt_inv, dx_inv, kk[k], h0[k],
+                                k < 3 ? h0[k + 1] : hE0, k < 3 ? s0[k + 1] : sE0, s0[k], qx0[k], qy0[k],
+                                k < 3 ? qy0[k + 1] : qyE0, qyS[k], k < 3 ? qyS[k + 1] : qySE);
+        const float gq = upd_qy(fy[k], k > 0 ? fy[k - 1] : fyW, gy0[k], gy1[k], dt, dx, dt_inv, dx_inv, kk[k], h0[k],
+                                h1[k], s1[k], s0[k], qy0[k], qx0[k], k > 0 ? qx0[k - 1] : qxW0, qx1[k],
+                                k > 0 ? qx1[k - 1] : qxW1);
+        qx2[k] = holdX[k] ? qx0[k] : fq;  // boundary-face holds (:373-376)
+        qy2[k] = hold_y ? qy0[k] : gq;
+      }
+      const float qx2W = __shfl_up_sync(0xffffffffu, qx2[3], 1);
+
+      if (r >= ra) {
+        const bool rowH = (r >= 1 && r <= H - 2);
+        const bool rowQX = (r >= 2 && r <= H - 3);
+        const bool rowQY = (r >= 1 && r <= H - 3);
+        float h2[4];
+        bool wH[4], wQX[4], wQY[4];
+        bool allH = true, allQX = true, allQY = true;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          h2[k] = h0[k] - dt * dx_inv * ((qx2[k] - (k > 0 ? qx2[k - 1] : qx2W)) + (qy2[k] - qy2S[k]));
+          const bool valid = (s0[k] != nv);
+          wH[k] = rowH && colH[k] && valid;
+          wQX[k] = rowQX && colQX[k] && valid;
+          wQY[k] = rowQY && colQY[k] && valid;
+          allH &= wH[k];
+          allQX &= wQX[k];
+          allQY &= wQY[k];
+          if (wH[k]) {
+            bad |= !(fabsf(h2[k]) <= 3.402823466e38f);
+            if (h2[k] > kEPS) {  // CFL of wet stored cells (:392-396), velocities of the old state
+              const float uw = k > 0 ? ux0[k - 1] : uxW0;
+              const float umax = fmaxf(fabsf(uy0[k]), fmaxf(fabsf(uyS[k]), fmaxf(fabsf(ux0[k]), fabsf(uw))));
+              const float dtc = dx / (sqrtf(kG * h2[k]) + umax);
+              cfl = fminf(cfl, dtc);
+            }
+          }
+          if (colIn[k]) nzf |= (h2[k] != 0.f) | (qx2[k] != 0.f) | (qy2[k] != 0.f);
+        }
+        const size_t row_off = (size_t)r * (size_t)pitch + (size_t)c;
+        if (allH) {
+          *reinterpret_cast<float4*>(h_out + row_off) = make_float4(h2[0], h2[1], h2[2], h2[3]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (wH[k]) h_out[row_off + k] = h2[k];
+        }
+        if (allQX) {
+          *reinterpret_cast<float4*>(qx_out + row_off) = make_float4(qx2[0], qx2[1], qx2[2], qx2[3]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (wQX[k]) qx_out[row_off + k] = qx2[k];
+        }
+        if (allQY) {
+          *reinterpret_cast<float4*>(qy_out + row_off) = make_float4(qy2[0], qy2[1], qy2[2], qy2[3]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (wQY[k]) qy_out[row_off + k] = qy2[k];
+        }
+        if (fold) {  // flood_plains_kernel on the post-boundary state of the last step (:254-262)
+          if (colIn[0] && colIn[3]) {
+            float4* hm = reinterpret_cast<float4*>(a.hmax + row_off);
+            float4 m = *hm;
+            m.x = fmaxf(m.x, h0[0]);
+            m.y = fmaxf(m.y, h0[1]);
+            m.z = fmaxf(m.z, h0[2]);
+            m.w = fmaxf(m.w, h0[3]);
+            *hm = m;
+          } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+              if (colIn[k]) a.hmax[row_off + k] = fmaxf(a.hmax[row_off + k], h0[k]);
+          }
+        }
+        // per-tile wet flag for the next plan, flushed at the tile's last row
+        if ((r + 1) % FIP_TILE_ROWS == 0 || r + 1 == rb) {
+          if (__any_sync(0xffffffffu, nzf) && lane == 0) nzs[s * a.n_ty + r / FIP_TILE_ROWS] = 1;
+          nzf = false;
+        }
+      }
+
+      // travel north (:408-433)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        qy2S[k] = qy2[k];
+        qyS[k] = qy0[k];
+        gxS[k] = gx[k];
+        uyS[k] = uy0[k];
+        h0[k] = h1[k];
+        h1[k] = h2r[k];
+        qx0[k] = qx1[k];
+        qy0[k] = qy1[k];
+        s0[k] = s1[k];
+        ux0[k] = ux1[k];
+        uy0[k] = uy1[k];
+        gy0[k] = gy1[k];
+      }
+      qySE = qyE0;
+      hE0 = hE1;
+      hE1 = hE2;
+      qxW0 = qxW1;
+      qyE0 = qyE1;
+      sE0 = sE1;
+      uxW0 = ux1W;
+      uyE0 = uy1E;
+    }
+    if (!ok) break;
+    release_row(rb);
+    release_row(rb + 1);
+    seq += (uint32_t)(rb - ra + 4);
+  }
+
+  // inactive tiles still fold hmax when the initial state had negative depths
+  if (fold && s_hdr[5]) {
+    const int ctid = tid;  // 0..127
+    for (int ch = 0; ch < a.n_chunks; ++ch) {
+      const int in_chunk = min(FIP_PLAN_CHUNK, a.n_tiles - ch * FIP_PLAN_CHUNK);
+      const int n_inact = in_chunk - (s_prefix[ch + 1] - s_prefix[ch]);
+      for (int i = blockIdx.x; i < n_inact; i += gridDim.x) {
+        const int tile = list[ch * FIP_PLAN_CHUNK + FIP_PLAN_CHUNK - 1 - i];
+        const int st = tile / a.n_ty, ty = tile - st * a.n_ty;
+        const int c0 = st * FIP_TILE_COLS, r0 = ty * FIP_TILE_ROWS;
+        for (int e = ctid; e < FIP_TILE_COLS * FIP_TILE_ROWS; e += kConsumerWarps * 32) {
+          const int rr = r0 + e / FIP_TILE_COLS, cc = c0 + e % FIP_TILE_COLS;
+          if (rr < H && cc < W) {
+            const size_t o = (size_t)rr * pitch + cc;
+            a.hmax[o] = fmaxf(a.hmax[o], h_in[o]);
+          }
+        }
+      }
+    }
+  }
+
+  // CFL minimum: warp reduction, one atomicMin per warp on the float bits (all positive)
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) cfl = fminf(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+  const bool any_bad = __any_sync(0xffffffffu, bad);
+  if (lane == 0) {
+    if (cfl < 1.0f) atomicMin(&ctl->cfl_bits[it & 1], __float_as_uint(cfl));
+    if (any_bad) ctl->nonfinite = 1;
+  }
+}
+
+__global__ void init_tiles_kernel(const float* h, const float* qx, const float* qy, const float* sohle, int W, int H,
+                                  int pitch, float no_value, int n_ty, int n_tiles, unsigned char* sticky,
+                                  unsigned char* nz0, unsigned char* nz1) {
+  const int t = blockIdx.x;
+  if (t >= n_tiles) return;
+  const int s = t / n_ty, ty = t - s * n_ty;
+  const int c0 = s * FIP_TILE_COLS, r0 = ty * FIP_TILE_ROWS;
+  const int c1 = min(c0 + FIP_TILE_COLS, W), r1 = min(r0 + FIP_TILE_ROWS, H);
+  int nz = 0, st = 0;
+  for (int e = threadIdx.x; e < FIP_TILE_COLS * FIP_TILE_ROWS; e += blockDim.x) {
+    const int r = r0 + e / FIP_TILE_COLS, c = c0 + e % FIP_TILE_COLS;
+    if (r < r1 && c < c1) {
+      const size_t o = (size_t)r * pitch + c;
+      const bool nzc = (h[o] != 0.f) || (qx[o] != 0.f) || (qy[o] != 0.f);
+      nz |= nzc;
+      if (sohle[o] == no_value && nzc) st = 1;  // never written by the step: static water
+    }
+  }
+  // border band: boundary conditions write within 2 cells of the edge and the stencil reads
+  // 2 cells further, so tiles reaching within 4 cells of an edge are always computed
+  if (r0 < 4 || r1 > H - 4 || c0 < 4 || c1 > W - 4) st = 1;
+  nz = __syncthreads_or(nz);
+  st = __syncthreads_or(st);
+  if (threadIdx.x == 0) {
+    sticky[t] = (unsigned char)st;
+    nz0[t] = (unsigned char)nz;
+    nz1[t] = (unsigned char)nz;
+  }
+}
+
+__global__ void hmax_fold_kernel(const float* __restrict__ h, float* __restrict__ hmax, int W, int H, int pitch) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (c >= W || r >= H) return;
+  const size_t o = (size_t)r * pitch + c;
+  hmax[o] = fmaxf(hmax[o], h[o]);
+}
+
+constexpr int kVolBlocks = 1184;  // 8 per SM on 148 SMs
+constexpr int kVolThreads = 256;
+
+__global__ void volume_partial_kernel(const float* __restrict__ h, int W, int H, int pitch, double* partials) {
+  __shared__ double red[kVolThreads];
+  double acc = 0.0;
+  for (int r = blockIdx.x; r < H; r += gridDim.x) {
+    const float* row = h + (size_t)r * pitch;
+    for (int c = threadIdx.x; c < W; c += blockDim.x) acc += (double)row[c];
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+}
+
+__global__ void volume_final_kernel(const double* partials, int n, double* out) {
+  __shared__ double red[kVolThreads];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partials[i];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+__global__ void sample_gather_kernel(const float* h, const float* qx, const float* qy, const float* sohle, int pitch,
+                                     int n, const int* xy_type, float* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int x = xy_type[3 * i], y = xy_type[3 * i + 1], t = xy_type[3 * i + 2];
+  const size_t o = (size_t)y * pitch + x;
+  float v;
+  if (t == 0) v = __fadd_rn(h[o], sohle[o]);  // sample(): val += h_sohle (src/main.cpp:62-67)
+  else if (t == 1) v = h[o];
+  else if (t == 2) v = qx[o];
+  else v = qy[o];
+  out[i] = v;
+}
+
+}  // namespace
+
+void tile_geometry(int W, int H, int* n_sx, int* n_ty, int* n_tiles, int* n_chunks) {
+  *n_sx = (W + FIP_TILE_COLS - 1) / FIP_TILE_COLS;
+  *n_ty = (H + FIP_TILE_ROWS - 1) / FIP_TILE_ROWS;
+  *n_tiles = *n_sx * *n_ty;
+  *n_chunks = (*n_tiles + FIP_PLAN_CHUNK - 1) / FIP_PLAN_CHUNK;
+}
+
+static int encode_map(CUtensorMap* tm, float* base, int W, int H, int pitch) {
+  cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)H};
+  cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
+  cuuint32_t box[2] = {256, 1};
+  cuuint32_t estr[2] = {1, 1};
+  if (!drv::TensorMapEncodeTiled) return (int)CUDA_ERROR_NOT_INITIALIZED;
+  CUresult r = drv::TensorMapEncodeTiled(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+                                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (int)r;
+}
+
+int make_tensor_maps(StencilState* st) {
+  int r = 0;
+  for (int b = 0; b < 2; ++b) {
+    if ((r = encode_map(&st->tm_h[b], st->h[b], st->W, st->H, st->pitch))) return r;
+    if ((r = encode_map(&st->tm_qx[b], st->qx[b], st->W, st->H, st->pitch))) return r;
+    if ((r = encode_map(&st->tm_qy[b], st->qy[b], st->W, st->H, st->pitch))) return r;
+  }
+  if ((r = encode_map(&st->tm_sohle, st->sohle, st->W, st->H, st->pitch))) return r;
+  if ((r = encode_map(&st->tm_kst, st->kst ? st->kst : st->sohle, st->W, st->H, st->pitch))) return r;
+  return 0;
+}
+
+int rmg_step_grid(int device) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return 2 * sms;
+}
+
+template <bool KVAR>
+static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t stream) {
+  constexpr int NF = KVAR ? 5 : 4;
+  const int smem = kNSlot * NF * kFieldBytes + 1024;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(rmg_step_kernel<KVAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  StepArgs a;
+  for (int b = 0; b < 2; ++b) {
+    a.h[b] = st.h[b];
+    a.qx[b] = st.qx[b];
+    a.qy[b] = st.qy[b];
+    a.list[b] = st.list[b];
+    a.chunk_cnt[b] = st.chunk_cnt[b];
+    a.nz[b] = st.nz[b];
+  }
+  a.hmax = st.hmax;
+  a.ctl = st.ctl;
+  a.W = st.W;
+  a.H = st.H;
+  a.pitch = st.pitch;
+  a.n_sx = st.n_sx;
+  a.n_ty = st.n_ty;
+  a.n_tiles = st.n_tiles;
+  a.n_chunks = st.n_chunks;
+  a.dx = st.dx;
+  a.kst_fixed = st.kst_fixed;
+  a.no_value = st.no_value;
+  rmg_step_kernel<KVAR><<<grid, kThreads, smem, stream>>>(st.tm_h[0], st.tm_h[1], st.tm_qx[0], st.tm_qx[1],
+                                                          st.tm_qy[0], st.tm_qy[1], st.tm_sohle, st.tm_kst, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t stream) {
+  if (st.n_chunks > kMaxChunks) return cudaErrorInvalidValue;
+  return st.kst ? launch_step_t<true>(st, grid, stream) : launch_step_t<false>(st, grid, stream);
+}
+
+cudaError_t launch_init_tiles(const StencilState& st, cudaStream_t stream) {
+  init_tiles_kernel<<<st.n_tiles, 256, 0, stream>>>(st.h[0], st.qx[0], st.qy[0], st.sohle, st.W, st.H, st.pitch,
+                                                    st.no_value, st.n_ty, st.n_tiles, st.sticky, st.nz[0], st.nz[1]);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hmax_fold(const StencilState& st, int parity, cudaStream_t stream) {
+  dim3 grid((st.W + 255) / 256, st.H);
+  hmax_fold_kernel<<<grid, 256, 0, stream>>>(st.h[parity], st.hmax, st.W, st.H, st.pitch);
+  return cudaGetLastError();
+}
+
+int volume_partials(const StencilState&) { return kVolBlocks; }
+
+cudaError_t launch_volume(const StencilState& st, int parity, double* partials, double* out, cudaStream_t stream) {
+  volume_partial_kernel<<<kVolBlocks, kVolThreads, 0, stream>>>(st.h[parity], st.W, st.H, st.pitch, partials);
+  volume_final_kernel<<<1, kVolThreads, 0, stream>>>(partials, kVolBlocks, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, const int* xy_type, float* out,
+                                 cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  sample_gather_kernel<<<(n + 127) / 128, 128, 0, stream>>>(st.h[parity], st.qx[parity], st.qy[parity], st.sohle,
+                                                            st.pitch, n, xy_type, out);
+  return cudaGetLastError();
+}
+
+}  // namespace fip

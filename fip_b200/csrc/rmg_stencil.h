@@ -1,0 +1,59 @@
+// Host interface of the sm_100a kernels in rmg_stencil.cu (internal to libfip_b200).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fip_ctl.h"
+
+namespace fip {
+
+// Device buffers and planning scratch of one scenario. Fields are cudaMallocPitch'ed like the
+// reference (src/simdata.cpp:63-73): W floats per row, H+3 rows, `pitch` elements per row.
+struct StencilState {
+  float* h[2];
+  float* qx[2];
+  float* qy[2];
+  float* sohle;
+  float* kst;   // nullptr: uniform kst_fixed
+  float* hmax;
+  FipCtl* ctl;  // device control block
+  unsigned char* sticky;  // per tile: always active (domain border band, static no_data water)
+  unsigned char* nz[2];   // per tile: some cell of the new state is nonzero, by iteration parity
+  int* list[2];           // active tiles by chunk (front) / inactive tiles (back), by parity
+  int* chunk_cnt[2];      // active tiles per chunk, by parity
+  int W, H, pitch;
+  int n_sx, n_ty, n_tiles, n_chunks;
+  float dx, kst_fixed, no_value;
+  CUtensorMap tm_h[2], tm_qx[2], tm_qy[2], tm_sohle, tm_kst;
+};
+
+// Geometry of the tile grid for a W x H domain.
+void tile_geometry(int W, int H, int* n_sx, int* n_ty, int* n_tiles, int* n_chunks);
+
+// Encodes the TMA descriptors of every field (box 256 x 1 floats). Returns a CUresult.
+int make_tensor_maps(StencilState* st);
+
+// One rmg step over the active tiles of the current plan (reads ctl on the device).
+cudaError_t launch_rmg_step(const StencilState& st, int grid_ctas, cudaStream_t stream);
+
+// Per-tile sticky flags and the nonzero flags of the initial state (both parities).
+cudaError_t launch_init_tiles(const StencilState& st, cudaStream_t stream);
+
+// hmax = max(hmax, h[parity]) over the whole grid (the reference's flood_plains_kernel).
+cudaError_t launch_hmax_fold(const StencilState& st, int parity, cudaStream_t stream);
+
+// FP64 sum of h[parity] over the grid into *out (device), deterministic order. `partials`
+// holds at least volume_partials() doubles.
+int volume_partials(const StencilState& st);
+cudaError_t launch_volume(const StencilState& st, int parity, double* partials, double* out,
+                          cudaStream_t stream);
+
+// Gathers n sample values (type 0..3 = z, h, qx, qy; z adds terrain) of buffer `parity`.
+cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, const int* xy_type,
+                                 float* out, cudaStream_t stream);
+
+// Number of CTAs the step kernel runs with (2 per SM).
+int rmg_step_grid(int device);
+
+}  // namespace fip

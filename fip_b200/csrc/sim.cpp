@@ -1,0 +1,789 @@
+// Simulation handle: device buffers, the batched step loop and the events of the reference's
+// simulate() (src/main.cpp:100-135), behind the C ABI of include/fip.h.
+//
+// A step is two launches on the handle's stream: the rmg stencil (rmg_stencil.cu) and the
+// NVRTC-built post kernel (bc_codegen.cpp). All per-step scalars stay on the device (FipCtl), so
+// batches of up to 64 steps run as one captured CUDA graph; the post kernel stops a batch
+// (ctl->stop) at the steps where the reference samples, dumps or ends the run, and the host
+// handles that event and resumes.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <functional>
+#include <iostream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "bc_codegen.h"
+#include "config.h"
+#include "drv.h"
+#include "fip.h"
+#include "fip_ctl.h"
+#include "rmg_stencil.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+void ckd(CUresult r, const char* what) {
+  if (r != CUDA_SUCCESS) throw CudaError(fip::drv::message(r, what));
+}
+
+constexpr double kInf = std::numeric_limits<double>::infinity();
+
+}  // namespace
+
+struct fip_handle {
+  fip::Config cfg;
+  fip_options opt;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  fip::StencilState st{};
+  fip::PostKernel post;
+  fip::SeriesLayout series;
+  float* d_series = nullptr;
+  FipCtl* d_ctl = nullptr;
+  FipCtl* h_ctl = nullptr;  // pinned mirror
+  double* d_vol_partials = nullptr;
+  double* d_vol = nullptr;
+  int* d_sample_idx = nullptr;
+  float* d_sample_val = nullptr;
+  float* h_sample_val = nullptr;
+  int grid_ctas = 0;
+  bool started = false;     // the iteration-0 boundary conditions have run
+  double sample_timer = 0;  // Sampling::timer
+  size_t save_pos = 0;
+  std::map<int, cudaGraphExec_t> graphs;
+  std::ostream* out = &std::cout;
+  std::unique_ptr<std::ofstream> out_file;
+
+  ~fip_handle();
+  void init(const std::string& yaml, const fip_options& o);
+  void write_ctl_fields();
+  void read_ctl();
+  void launch_post(int mode);
+  void launch_step_pair();
+  void launch_batch(int k);
+  int run_steps(long long budget, bool to_target);
+  void sample();
+  void dump(const std::string& prefix, bool current);
+  void flush_hmax_if_due();
+  int steps_hint() const;
+};
+
+fip_handle::~fip_handle() {
+  if (device >= 0) cudaSetDevice(device);
+  for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+  fip::destroy_post_kernel(&post);
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(st.h[b]);
+    cudaFree(st.qx[b]);
+    cudaFree(st.qy[b]);
+    cudaFree(st.nz[b]);
+    cudaFree(st.list[b]);
+    cudaFree(st.chunk_cnt[b]);
+  }
+  cudaFree(st.sohle);
+  cudaFree(st.kst);
+  cudaFree(st.hmax);
+  cudaFree(st.sticky);
+  cudaFree(d_series);
+  cudaFree(d_ctl);
+  cudaFree(d_vol_partials);
+  cudaFree(d_vol);
+  cudaFree(d_sample_idx);
+  cudaFree(d_sample_val);
+  if (h_ctl) cudaFreeHost(h_ctl);
+  if (h_sample_val) cudaFreeHost(h_sample_val);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void fip_handle::init(const std::string& yaml, const fip_options& o) {
+  opt = o;
+  device = o.device;
+  ck(cudaSetDevice(device), "cudaSetDevice");
+  ck(cudaFree(nullptr), "CUDA context");
+  std::string derr;
+  if (!fip::drv::load(&derr)) throw CudaError(derr);
+  ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  const size_t W = cfg.W, H = cfg.H;
+  const size_t row_bytes = W * sizeof(float);
+  size_t pitch_bytes = 0;
+  // initDeviceBuffers (src/simdata.cpp:54-96): pitched fields of H+3 rows
+  auto alloc_field = [&](float** p) {
+    size_t pb = 0;
+    ck(cudaMallocPitch((void**)p, &pb, row_bytes, H + 3), "cudaMallocPitch");
+    if (pitch_bytes && pb != pitch_bytes) throw CudaError("inconsistent pitch");
+    pitch_bytes = pb;
+    ck(cudaMemset2D(*p, pb, 0, row_bytes, H + 3), "cudaMemset2D");
+  };
+  for (int b = 0; b < 2; ++b) {
+    alloc_field(&st.h[b]);
+    alloc_field(&st.qx[b]);
+    alloc_field(&st.qy[b]);
+  }
+  alloc_field(&st.sohle);
+  alloc_field(&st.hmax);
+  if (cfg.has_kst_var) alloc_field(&st.kst);
+  if (pitch_bytes % 16) throw CudaError("row pitch is not a multiple of 16 bytes");
+  const int pitch = (int)(pitch_bytes / sizeof(float));
+  auto up = [&](float* dst, const std::vector<float>& src) {
+    ck(cudaMemcpy2D(dst, pitch_bytes, src.data(), row_bytes, row_bytes, H, cudaMemcpyHostToDevice), "cudaMemcpy2D");
+  };
+  for (int b = 0; b < 2; ++b) {
+    up(st.h[b], cfg.h0);
+    up(st.qx[b], cfg.qx0);
+    up(st.qy[b], cfg.qy0);
+  }
+  up(st.hmax, cfg.h0);
+  up(st.sohle, cfg.terrain);
+  if (cfg.has_kst_var) up(st.kst, cfg.kst);
+
+  st.W = (int)W;
+  st.H = (int)H;
+  st.pitch = pitch;
+  st.dx = cfg.dx;
+  st.kst_fixed = cfg.kst_fixed;
+  st.no_value = cfg.no_data;
+  fip::tile_geometry(st.W, st.H, &st.n_sx, &st.n_ty, &st.n_tiles, &st.n_chunks);
+  if (st.n_chunks > 256) throw CudaError("grid too large: more than 131072 tiles");
+  ck(cudaMalloc((void**)&st.sticky, st.n_tiles), "cudaMalloc");
+  for (int b = 0; b < 2; ++b) {
+    ck(cudaMalloc((void**)&st.nz[b], st.n_tiles), "cudaMalloc");
+    ck(cudaMalloc((void**)&st.list[b], sizeof(int) * st.n_chunks * FIP_PLAN_CHUNK), "cudaMalloc");
+    ck(cudaMalloc((void**)&st.chunk_cnt[b], sizeof(int) * st.n_chunks), "cudaMalloc");
+    ck(cudaMemset(st.chunk_cnt[b], 0, sizeof(int) * st.n_chunks), "cudaMemset");
+  }
+  ck(cudaMalloc((void**)&d_ctl, sizeof(FipCtl)), "cudaMalloc");
+  st.ctl = d_ctl;
+  ckd((CUresult)fip::make_tensor_maps(&st), "cuTensorMapEncodeTiled");
+
+  series = fip::layout_series(cfg);
+  ck(cudaMalloc((void**)&d_series, series.data.size() * sizeof(float)), "cudaMalloc");
+  ck(cudaMemcpy(d_series, series.data.data(), series.data.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
+
+  const int vp = fip::volume_partials(st);
+  ck(cudaMalloc((void**)&d_vol_partials, sizeof(double) * vp), "cudaMalloc");
+  ck(cudaMalloc((void**)&d_vol, sizeof(double)), "cudaMalloc");
+  const int np = (int)cfg.points.size();
+  if (np) {
+    std::vector<int> idx;
+    for (const auto& p : cfg.points) {
+      idx.push_back(p.x);
+      idx.push_back(p.y);
+      idx.push_back((int)p.type);
+    }
+    ck(cudaMalloc((void**)&d_sample_idx, sizeof(int) * idx.size()), "cudaMalloc");
+    ck(cudaMemcpy(d_sample_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+    ck(cudaMalloc((void**)&d_sample_val, sizeof(float) * np), "cudaMalloc");
+    ck(cudaMallocHost((void**)&h_sample_val, sizeof(float) * np), "cudaMallocHost");
+  }
+
+  // control block
+  ck(cudaMallocHost((void**)&h_ctl, sizeof(FipCtl)), "cudaMallocHost");
+  std::memset(h_ctl, 0, sizeof(FipCtl));
+  h_ctl->duration = 0.0;
+  h_ctl->next_sample = kInf;
+  h_ctl->next_save = cfg.save_times.empty() ? kInf : cfg.save_times[0];
+  h_ctl->target = kInf;
+  h_ctl->dt = cfg.dt;
+  h_ctl->last_cfl = 1.0f;
+  h_ctl->variable_dt = cfg.variable_dt ? 1 : 0;
+  h_ctl->stop_on_nonfinite = opt.stop_on_nonfinite ? 1 : 0;
+  h_ctl->hmax_every = 100;
+  bool negative = false;
+  for (float v : cfg.h0) negative |= (v < 0.f);
+  h_ctl->hmax_full = negative ? 1 : 0;
+  h_ctl->force_all = opt.all_tiles ? 1 : 0;
+  const float one = 1.0f;
+  std::memcpy(&h_ctl->cfl_bits[0], &one, 4);
+  std::memcpy(&h_ctl->cfl_bits[1], &one, 4);
+  if (cfg.variable_dt) {
+    // controlTimestep at the start of the first simulate(): the CFL slots hold 1 (src/simdata.cpp:91-94)
+    float min_cfl = 42.0f;
+    if (1.0f < min_cfl) min_cfl = 1.0f;
+    const float target = min_cfl * .5f, dc = 0.001f;
+    float d = h_ctl->dt;
+    if (d < target && target - d > dc) d *= 1.001f;
+    else if (d > target && d - target > dc) d *= 0.99f;
+    h_ctl->dt = d;
+  }
+  ck(cudaMemcpy(d_ctl, h_ctl, sizeof(FipCtl), cudaMemcpyHostToDevice), "cudaMemcpy");
+  ck(fip::launch_init_tiles(st, stream), "init_tiles");
+  grid_ctas = fip::rmg_step_grid(device);
+
+  // boundary-condition program (BoundaryConditionKernel::generate)
+  std::string err;
+  std::string src = fip::post_kernel_source(cfg, series, pitch);
+  if (fip::build_post_kernel(src, &post, &err)) throw std::invalid_argument("NVRTC:" + err);
+  ck(cudaStreamSynchronize(stream), "init");
+
+  if (opt.quiet) {
+    out = nullptr;
+  } else if (opt.sample_path) {
+    out_file.reset(new std::ofstream(opt.sample_path));
+    if (!*out_file) throw std::invalid_argument(std::string("IO:cannot open ") + opt.sample_path);
+    out = out_file.get();
+  }
+  if (out && !cfg.points.empty()) {  // sampleHeader (src/main.cpp:45-51)
+    *out << "t;";
+    for (const auto& p : cfg.points) *out << p.label << ";";
+    *out << std::endl;
+  }
+}
+
+// host-owned control fields: event times, step budget, stop flag
+void fip_handle::write_ctl_fields() {
+  const size_t off = offsetof(FipCtl, duration);
+  (void)off;
+  // the device owns duration/dt/iteration/parity; write only the fields the host controls
+  auto put = [&](size_t offset, size_t bytes) {
+    ck(cudaMemcpyAsync(reinterpret_cast<char*>(d_ctl) + offset, reinterpret_cast<char*>(h_ctl) + offset, bytes,
+                       cudaMemcpyHostToDevice, stream),
+       "ctl upload");
+  };
+  put(offsetof(FipCtl, next_sample), 3 * sizeof(double));  // next_sample, next_save, target
+  put(offsetof(FipCtl, stop), 3 * sizeof(int));            // stop, stop_reason, steps_left
+}
+
+void fip_handle::read_ctl() {
+  ck(cudaMemcpyAsync(h_ctl, d_ctl, sizeof(FipCtl), cudaMemcpyDeviceToHost, stream), "ctl download");
+  ck(cudaStreamSynchronize(stream), "step");
+}
+
+void fip_handle::launch_post(int mode) {
+  FipPostArgs a;
+  std::memset(&a, 0, sizeof a);
+  for (int b = 0; b < 2; ++b) {
+    a.h[b] = st.h[b];
+    a.qx[b] = st.qx[b];
+    a.qy[b] = st.qy[b];
+    a.nz[b] = st.nz[b];
+    a.list[b] = st.list[b];
+    a.chunk_cnt[b] = st.chunk_cnt[b];
+  }
+  a.sohle = st.sohle;
+  a.ctl = d_ctl;
+  a.sticky = st.sticky;
+  a.series = d_series;
+  a.W = st.W;
+  a.H = st.H;
+  a.pitch = st.pitch;
+  a.n_sx = st.n_sx;
+  a.n_ty = st.n_ty;
+  a.n_tiles = st.n_tiles;
+  a.n_chunks = st.n_chunks;
+  a.mode = mode;
+  a.dx = st.dx;
+  void* params[] = {&a};
+  ckd(fip::drv::LaunchKernel(post.fn, 1 + st.n_chunks, 1, 1, FIP_POST_THREADS, 1, 1, 0, (CUstream)stream, params, nullptr),
+      "fip_post launch");
+}
+
+void fip_handle::launch_step_pair() {
+  ck(fip::launch_rmg_step(st, grid_ctas, stream), "rmg_step launch");
+  launch_post(FIP_POST_MODE_STEP);
+}
+
+void fip_handle::launch_batch(int k) {
+  if (!opt.use_graphs || k == 1) {
+    for (int i = 0; i < k; ++i) launch_step_pair();
+    return;
+  }
+  auto it = graphs.find(k);
+  if (it == graphs.end()) {
+    cudaGraph_t g;
+    ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
+    for (int i = 0; i < k; ++i) launch_step_pair();
+    ck(cudaStreamEndCapture(stream, &g), "capture");
+    cudaGraphExec_t ex;
+    ck(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate");
+    cudaGraphDestroy(g);
+    it = graphs.emplace(k, ex).first;
+  }
+  ck(cudaGraphLaunch(it->second, stream), "cudaGraphLaunch");
+}
+
+// Steps until the next event can end a batch: exact for fixed dt (same double accumulation as
+// the device), a lower estimate for variable dt.
+int fip_handle::steps_hint() const {
+  double next = std::min(h_ctl->next_sample, std::min(h_ctl->next_save, h_ctl->target));
+  const long long budget = h_ctl->steps_left;
+  long long n = budget;
+  if (next < kInf) {
+    double d = h_ctl->duration;
+    long long j = 0;
+    if (!cfg.variable_dt) {
+      const float dt = h_ctl->dt;
+      while (j < 64 && d < next) {
+        d += dt;
+        ++j;
+      }
+      if (d < next) j = 64;
+    } else {
+      const double dtmax = (double)h_ctl->dt * 1.07;  // at most +0.1% per step over 64 steps
+      j = dtmax > 0 ? (long long)((next - d) / dtmax) : 1;
+      if (j < 1) j = 1;
+    }
+    n = std::min(n, j);
+  }
+  if (n > 64) n = 64;
+  if (n < 1) n = 1;
+  int k = 1;
+  while (k * 2 <= n) k *= 2;
+  return k;
+}
+
+void fip_handle::flush_hmax_if_due() {
+  if (h_ctl->iteration > 0 && h_ctl->iteration % h_ctl->hmax_every == 0)
+    ck(fip::launch_hmax_fold(st, h_ctl->parity, stream), "hmax");
+}
+
+void fip_handle::sample() {  // sample (src/main.cpp:53-83)
+  if (!out) return;
+  const int np = (int)cfg.points.size();
+  if (np) {
+    ck(fip::launch_sample_gather(st, h_ctl->parity, np, d_sample_idx, d_sample_val, stream), "sample");
+    ck(cudaMemcpyAsync(h_sample_val, d_sample_val, sizeof(float) * np, cudaMemcpyDeviceToHost, stream), "sample");
+    ck(cudaStreamSynchronize(stream), "sample");
+  }
+  *out << h_ctl->duration << ";";
+  for (int i = 0; i < np; ++i) *out << h_sample_val[i] << ";";
+  *out << std::endl;
+}
+
+void fip_handle::dump(const std::string& prefix, bool current) {
+  // dumpDeviceBuffers (src/main.cpp:180-202)
+  ck(cudaStreamSynchronize(stream), "dump");
+  const size_t W = cfg.W, H = cfg.H;
+  std::vector<float> buf(W * H);
+  char stamp[64];
+  std::time_t now = std::time(nullptr);
+  std::tm tmv;
+  gmtime_r(&now, &tmv);
+  std::strftime(stamp, sizeof stamp, "%Y-%m-%d-%H-%M", &tmv);
+  const int b = current ? h_ctl->parity : (h_ctl->parity ^ 1);
+  const float* src[4] = {st.h[b], st.qx[b], st.qy[b], st.hmax};
+  const char* tag[4] = {"_ah_", "_qx_", "_qy_", "_flood_plains_"};
+  for (int f = 0; f < 4; ++f) {
+    ck(cudaMemcpy2D(buf.data(), W * 4, src[f], (size_t)st.pitch * 4, W * 4, H, cudaMemcpyDeviceToHost), "dump");
+    std::string fn = prefix + tag[f] + std::to_string((int)h_ctl->duration) + "_" + stamp;
+    std::ofstream file(fn, std::ios::binary);
+    if (!file) throw std::invalid_argument("IO:Failed to open file " + fn);
+    size_t w = W, hh = H;
+    file.write(reinterpret_cast<const char*>(&w), sizeof(size_t));
+    file.write(reinterpret_cast<const char*>(&hh), sizeof(size_t));
+    file.write(reinterpret_cast<const char*>(buf.data()), (std::streamsize)(W * H * sizeof(float)));
+    if (!file) throw std::invalid_argument("IO:write failed: " + fn);
+  }
+}
+
+// Runs up to `budget` simulate() calls (or until target_duration when to_target).
+int fip_handle::run_steps(long long budget, bool to_target) {
+  ck(cudaSetDevice(device), "cudaSetDevice");
+  if (to_target && h_ctl->duration >= cfg.target_duration) return FIP_OK;
+  if (budget <= 0) return FIP_OK;
+  if (!started) {
+    // start of the first simulate(): sampling before the iteration-0 boundary conditions
+    if (h_ctl->duration >= sample_timer && cfg.sampling_interval > 0) {
+      sample_timer += cfg.sampling_interval;
+      sample();
+    }
+    h_ctl->next_sample = cfg.sampling_interval > 0 ? sample_timer : kInf;
+    h_ctl->stop = 0;
+    h_ctl->stop_reason = 0;
+    h_ctl->steps_left = 1;
+    write_ctl_fields();
+    launch_post(FIP_POST_MODE_INIT);
+    started = true;
+  }
+  h_ctl->target = to_target ? cfg.target_duration : kInf;
+  h_ctl->steps_left = budget > (1LL << 30) ? (1 << 30) : (int)budget;
+  h_ctl->stop = 0;
+  h_ctl->stop_reason = 0;
+  write_ctl_fields();
+  const int it0 = h_ctl->iteration;
+  int rc = FIP_OK;
+  for (;;) {
+    launch_batch(steps_hint());
+    read_ctl();
+    if (h_ctl->error) return fail(FIP_ERR_DEVICE_TIMEOUT, "device wait ran out (code " + std::to_string(h_ctl->error) + ")");
+    const int reason = h_ctl->stop ? h_ctl->stop_reason : 0;
+    bool done = false;
+    if (reason & FIP_STOP_SAVE) {  // end of simulate(): dump after hmax
+      flush_hmax_if_due();
+      ++save_pos;
+      dump(cfg.name, false);
+      h_ctl->next_save = save_pos < cfg.save_times.size() ? cfg.save_times[save_pos] : kInf;
+    }
+    if (reason & FIP_STOP_TARGET) done = true;
+    if ((reason & FIP_STOP_SAMPLE) && !done) {  // start of the next simulate()
+      sample_timer += cfg.sampling_interval;
+      sample();
+      h_ctl->next_sample = sample_timer;
+    }
+    if (reason & FIP_STOP_NONFINITE) {
+      rc = fail(FIP_ERR_NONFINITE, "a stored water depth is NaN or Inf at iteration " + std::to_string(h_ctl->iteration));
+      done = true;
+    }
+    if (reason & FIP_STOP_BUDGET) done = true;
+    const long long ran = h_ctl->iteration - it0;
+    if (!done && !to_target && ran >= budget) done = true;
+    h_ctl->stop = 0;
+    h_ctl->stop_reason = 0;
+    h_ctl->steps_left = to_target ? (1 << 30) : (int)(budget - ran);
+    write_ctl_fields();
+    if (done) break;
+  }
+  flush_hmax_if_due();
+  ck(cudaStreamSynchronize(stream), "step");
+  return rc;
+}
+
+// ------------------------------------------------------------------------------------------
+namespace {
+
+int guard(const std::function<int()>& f) {
+  try {
+    return f();
+  } catch (const CudaError& e) {
+    return fail(FIP_ERR_CUDA, e.what());
+  } catch (const std::invalid_argument& e) {
+    std::string m = e.what();
+    if (m.rfind("IO:", 0) == 0) return fail(FIP_ERR_IO, m.substr(3));
+    if (m.rfind("NVRTC:", 0) == 0) return fail(FIP_ERR_NVRTC, m.substr(6));
+    return fail(FIP_ERR_CONFIG, m);
+  } catch (const std::exception& e) {
+    return fail(FIP_ERR_CUDA, e.what());
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void fip_default_options(fip_options* o) {
+  std::memset(o, 0, sizeof *o);
+  o->device = 0;
+  o->use_graphs = 1;
+}
+
+int fip_init_ex(const char* yaml_path, const fip_options* opt, fip_handle** out) {
+  if (!yaml_path || !out) return fail(FIP_ERR_ARG, "null argument");
+  *out = nullptr;
+  g_last_error.clear();
+  fip_options o;
+  fip_default_options(&o);
+  if (opt) o = *opt;
+  std::unique_ptr<fip_handle> h(new fip_handle());
+  std::string err;
+  int rc = fip::load_config(yaml_path, &h->cfg, &err);
+  if (rc == 2) return fail(FIP_ERR_IO, err);
+  if (rc) return fail(FIP_ERR_CONFIG, err);
+  rc = guard([&] {
+    h->init(yaml_path, o);
+    return FIP_OK;
+  });
+  if (rc) return rc;
+  *out = h.release();
+  return FIP_OK;
+}
+
+int fip_init(const char* yaml_path, fip_handle** out) { return fip_init_ex(yaml_path, nullptr, out); }
+
+int fip_step(fip_handle* h, int n) {
+  if (!h || n < 0) return fail(FIP_ERR_ARG, "bad argument");
+  return guard([&] { return h->run_steps(n, false); });
+}
+
+int fip_run(fip_handle* h) {
+  if (!h) return fail(FIP_ERR_ARG, "null handle");
+  return guard([&] { return h->run_steps(std::numeric_limits<long long>::max(), true); });
+}
+
+int fip_save(fip_handle* h, const char* prefix) {
+  if (!h) return fail(FIP_ERR_ARG, "null handle");
+  return guard([&] {
+    h->dump(prefix ? prefix : h->cfg.name, false);
+    return FIP_OK;
+  });
+}
+
+int fip_save_current(fip_handle* h, const char* prefix) {
+  if (!h) return fail(FIP_ERR_ARG, "null handle");
+  return guard([&] {
+    h->dump(prefix ? prefix : h->cfg.name, true);
+    return FIP_OK;
+  });
+}
+
+int fip_sample(fip_handle* h) {
+  if (!h) return fail(FIP_ERR_ARG, "null handle");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    h->sample();
+    return FIP_OK;
+  });
+}
+
+int fip_volume(fip_handle* h, double* outv) {
+  if (!h || !outv) return fail(FIP_ERR_ARG, "null argument");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    ck(fip::launch_volume(h->st, h->h_ctl->parity, h->d_vol_partials, h->d_vol, h->stream), "volume");
+    double v = 0;
+    ck(cudaMemcpyAsync(&v, h->d_vol, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "volume");
+    ck(cudaStreamSynchronize(h->stream), "volume");
+    *outv = v * (double)h->cfg.dx * (double)h->cfg.dx;
+    return FIP_OK;
+  });
+}
+
+int fip_get_field(fip_handle* h, int field, float* dst) {
+  if (!h || !dst) return fail(FIP_ERR_ARG, "null argument");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    const int p = h->h_ctl->parity;
+    const float* src = nullptr;
+    switch (field) {
+      case FIP_FIELD_H: src = h->st.h[p]; break;
+      case FIP_FIELD_QX: src = h->st.qx[p]; break;
+      case FIP_FIELD_QY: src = h->st.qy[p]; break;
+      case FIP_FIELD_HMAX: src = h->st.hmax; break;
+      case FIP_FIELD_H_PREV: src = h->st.h[p ^ 1]; break;
+      case FIP_FIELD_QX_PREV: src = h->st.qx[p ^ 1]; break;
+      case FIP_FIELD_QY_PREV: src = h->st.qy[p ^ 1]; break;
+      case FIP_FIELD_TERRAIN: src = h->st.sohle; break;
+      case FIP_FIELD_Z: src = h->st.h[p]; break;
+      default: return fail(FIP_ERR_ARG, "unknown field " + std::to_string(field));
+    }
+    const size_t W = h->cfg.W, H = h->cfg.H;
+    ck(cudaMemcpy2DAsync(dst, W * 4, src, (size_t)h->st.pitch * 4, W * 4, H, cudaMemcpyDeviceToHost, h->stream),
+       "fip_get_field");
+    ck(cudaStreamSynchronize(h->stream), "fip_get_field");
+    if (field == FIP_FIELD_Z)
+      for (size_t i = 0; i < W * H; ++i) dst[i] += h->cfg.terrain[i];
+    return FIP_OK;
+  });
+}
+
+int fip_time(fip_handle* h, double* duration, float* dt, int* iteration) {
+  if (!h) return fail(FIP_ERR_ARG, "null handle");
+  if (duration) *duration = h->h_ctl->duration;
+  if (dt) *dt = h->h_ctl->dt;
+  if (iteration) *iteration = h->h_ctl->iteration;
+  return FIP_OK;
+}
+
+int fip_info(fip_handle* h, fip_info_t* o) {
+  if (!h || !o) return fail(FIP_ERR_ARG, "null argument");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    std::memset(o, 0, sizeof *o);
+    o->W = h->st.W;
+    o->H = h->st.H;
+    o->pitch = h->st.pitch;
+    o->n_tiles = h->st.n_tiles;
+    if (h->started) {
+      std::vector<int> cnt(h->st.n_chunks);
+      ck(cudaMemcpy(cnt.data(), h->st.chunk_cnt[h->h_ctl->iteration & 1], sizeof(int) * cnt.size(),
+                    cudaMemcpyDeviceToHost),
+         "fip_info");
+      for (int c : cnt) o->active_tiles += c;
+    } else {
+      o->active_tiles = -1;
+    }
+    o->iteration = h->h_ctl->iteration;
+    o->duration = h->h_ctl->duration;
+    o->dt = h->h_ctl->dt;
+    o->last_cfl = h->h_ctl->last_cfl;
+    o->nonfinite = h->h_ctl->nonfinite;
+    return FIP_OK;
+  });
+}
+
+int fip_profile_steps(fip_handle* h, int n, float* stencil_ms, float* post_ms) {
+  if (!h || n <= 0) return fail(FIP_ERR_ARG, "bad argument");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    if (!h->started) {
+      int rc = h->run_steps(1, false);
+      if (rc) return rc;
+    }
+    h->h_ctl->target = kInf;
+    h->h_ctl->next_sample = kInf;  // profiling steps skip sampling and saves
+    const double save_keep = h->h_ctl->next_save;
+    h->h_ctl->next_save = kInf;
+    h->h_ctl->steps_left = n;
+    h->h_ctl->stop = 0;
+    h->h_ctl->stop_reason = 0;
+    h->write_ctl_fields();
+    std::vector<cudaEvent_t> ev(3 * n);
+    for (auto& e : ev) ck(cudaEventCreate(&e), "event");
+    for (int i = 0; i < n; ++i) {
+      ck(cudaEventRecord(ev[3 * i], h->stream), "event");
+      ck(fip::launch_rmg_step(h->st, h->grid_ctas, h->stream), "rmg_step");
+      ck(cudaEventRecord(ev[3 * i + 1], h->stream), "event");
+      h->launch_post(FIP_POST_MODE_STEP);
+      ck(cudaEventRecord(ev[3 * i + 2], h->stream), "event");
+    }
+    h->read_ctl();
+    double s = 0, p = 0;
+    for (int i = 0; i < n; ++i) {
+      float a = 0, b = 0;
+      ck(cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]), "event");
+      ck(cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]), "event");
+      s += a;
+      p += b;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (stencil_ms) *stencil_ms = (float)(s / n);
+    if (post_ms) *post_ms = (float)(p / n);
+    h->h_ctl->next_save = save_keep;
+    h->h_ctl->next_sample = h->cfg.sampling_interval > 0 ? h->sample_timer : kInf;
+    h->h_ctl->stop = 0;
+    h->h_ctl->stop_reason = 0;
+    h->write_ctl_fields();
+    ck(cudaStreamSynchronize(h->stream), "profile");
+    return FIP_OK;
+  });
+}
+
+void fip_destroy(fip_handle* h) { delete h; }
+
+const char* fip_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"
+
+// ---- host-only entry points ---------------------------------------------------------------
+namespace {
+
+std::string json_str(const std::string& s) {
+  std::string r = "\"";
+  for (char c : s) {
+    if (c == '"' || c == '\\') r += '\\';
+    if (c == '\n') {
+      r += "\\n";
+      continue;
+    }
+    r += c;
+  }
+  return r + "\"";
+}
+
+std::string json_num(double v) {
+  if (std::isnan(v)) return "\"nan\"";
+  if (std::isinf(v)) return v > 0 ? "\"inf\"" : "\"-inf\"";
+  char b[64];
+  std::snprintf(b, sizeof b, "%.17g", v);
+  return b;
+}
+
+int copy_out(const std::string& s, char* buf, int buflen) {
+  if (buf && buflen > 0) {
+    const int n = (int)std::min<size_t>(s.size(), (size_t)buflen - 1);
+    std::memcpy(buf, s.data(), n);
+    buf[n] = '\0';
+  }
+  return (int)s.size();
+}
+
+int load_for_host(const char* path, fip::Config* c) {
+  if (!path) return fail(FIP_ERR_ARG, "null path");
+  std::string err;
+  const int rc = fip::load_config(path, c, &err);
+  if (rc == 2) return fail(FIP_ERR_IO, err);
+  if (rc) return fail(FIP_ERR_CONFIG, err);
+  return FIP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fip_validate(const char* yaml_path) {
+  fip::Config c;
+  return load_for_host(yaml_path, &c);
+}
+
+int fip_config_json(const char* yaml_path, char* buf, int buflen) {
+  fip::Config c;
+  int rc = load_for_host(yaml_path, &c);
+  if (rc) return rc;
+  static const char* sides[] = {"left", "right", "top", "bottom"};
+  static const char* types[] = {"z", "q", "close", "open"};
+  static const char* stypes[] = {"z", "h", "qx", "qy"};
+  std::ostringstream o;
+  o << "{\"name\":" << json_str(c.name) << ",\"W\":" << c.W << ",\"H\":" << c.H << ",\"dx\":" << json_num(c.dx)
+    << ",\"dt\":" << json_num(c.dt) << ",\"variable_dt\":" << (c.variable_dt ? "true" : "false")
+    << ",\"solver\":" << (c.solver == fip::Solver::rmg ? "\"rmg\"" : "\"cn\"")
+    << ",\"target_duration\":" << json_num(c.target_duration) << ",\"kSt\":" << json_num(c.kst_fixed)
+    << ",\"no_data\":" << json_num(c.no_data) << ",\"kst_var\":" << (c.has_kst_var ? "true" : "false");
+  double hsum = 0;
+  for (float v : c.h0) hsum += v;
+  o << ",\"h0_sum\":" << json_num(hsum) << ",\"boundary_conditions\":[";
+  for (size_t i = 0; i < c.bcs.size(); ++i) {
+    const auto& b = c.bcs[i];
+    o << (i ? "," : "") << "{\"side\":\"" << sides[(int)b.side] << "\",\"type\":\"" << types[(int)b.type]
+      << "\",\"from\":" << b.from << ",\"to\":" << b.to << ",\"series\":" << (b.is_series ? "true" : "false")
+      << ",\"z\":" << json_num(b.z) << ",\"q\":" << json_num(b.q);
+    if (!b.is_series) o << ",\"qval\":" << json_num(c.const_q(b));
+    auto ts = [&](const char* k, const fip::TimeSeries& t, bool has) {
+      if (!has) return;
+      o << ",\"" << k << "_t\":[";
+      for (size_t j = 0; j < t.t.size(); ++j) o << (j ? "," : "") << json_num(t.t[j]);
+      o << "],\"" << k << "_v\":[";
+      for (size_t j = 0; j < t.v.size(); ++j) o << (j ? "," : "") << json_num(t.v[j]);
+      o << "]";
+    };
+    ts("z", b.z_series, b.has_z_series);
+    ts("q", b.q_series, b.has_q_series);
+    o << "}";
+  }
+  o << "],\"sampling_interval\":" << c.sampling_interval << ",\"sampling\":[";
+  for (size_t i = 0; i < c.points.size(); ++i)
+    o << (i ? "," : "") << "{\"x\":" << c.points[i].x << ",\"y\":" << c.points[i].y
+      << ",\"label\":" << json_str(c.points[i].label) << ",\"type\":\"" << stypes[(int)c.points[i].type] << "\"}";
+  o << "],\"save_state\":[";
+  for (size_t i = 0; i < c.save_times.size(); ++i) o << (i ? "," : "") << json_num(c.save_times[i]);
+  o << "]}";
+  return copy_out(o.str(), buf, buflen);
+}
+
+int fip_bc_program(const char* yaml_path, int pitch, int compile, char* buf, int buflen) {
+  fip::Config c;
+  int rc = load_for_host(yaml_path, &c);
+  if (rc) return rc;
+  if (pitch < (int)c.W) return fail(FIP_ERR_ARG, "pitch smaller than W");
+  fip::SeriesLayout ser = fip::layout_series(c);
+  std::string src = fip::post_kernel_source(c, ser, pitch);
+  if (compile) {
+    std::string cubin, log, err;
+    if (fip::compile_post_kernel(src, &cubin, &log, &err)) return fail(FIP_ERR_NVRTC, err);
+  }
+  return copy_out(src, buf, buflen);
+}
+
+}  // extern "C"

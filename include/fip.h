@@ -1,0 +1,140 @@
+/*
+ * fip_b200 -- C ABI of the B200 (sm_100a) slim shallow-water solver.
+ *
+ * Drop-in for the simulation loop of fip (fip-ems/fip). The reference has no library
+ * interface: its path sits behind globals in namespace SimData (src/simdata.h:333-373) and the
+ * functions cited below. Each entry point here replaces the reference code named in its
+ * comment, with the same inputs (the YAML parameter file and raw float32 grids of README.md:46-64)
+ * and the same outputs (sampling CSV on stdout, save_state dump files).
+ *
+ * Conventions: every function returns FIP_OK (0) or a negative FIP_ERR_* code and never exits
+ * the process; fip_last_error() gives the message of the last failure on the calling thread.
+ * A handle owns all device and host memory and one CUDA stream; handles are independent, and a
+ * handle is used from one thread at a time. Grids are row-major W x H float32 (row = y, north =
+ * +1 row; col = x, east = +1), unpitched on the host side.
+ */
+#ifndef FIP_B200_FIP_H
+#define FIP_B200_FIP_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FIP_OK 0
+#define FIP_ERR_CONFIG -1          /* invalid parameter file (the reference prints "Config error: ...") */
+#define FIP_ERR_IO -2              /* missing or short input file, unwritable dump */
+#define FIP_ERR_CUDA -3            /* CUDA runtime / driver error */
+#define FIP_ERR_NVRTC -4           /* boundary-condition kernel failed to compile */
+#define FIP_ERR_NONFINITE -5       /* a stored depth became NaN/Inf (only with stop_on_nonfinite) */
+#define FIP_ERR_DEVICE_TIMEOUT -6  /* a bounded device-side wait ran out; the handle is unusable */
+#define FIP_ERR_ARG -7             /* bad argument */
+
+/* fields for fip_get_field */
+#define FIP_FIELD_H 0        /* water depth of the current state (d_h1) */
+#define FIP_FIELD_QX 1       /* discharge on the east face of each cell (d_qx1) */
+#define FIP_FIELD_QY 2       /* discharge on the north face (d_qy1) */
+#define FIP_FIELD_HMAX 3     /* flood-plain (maximum depth) map (d_hmax) */
+#define FIP_FIELD_H_PREV 4   /* the ping-pong partner buffers (d_h2, d_qx2, d_qy2): the state */
+#define FIP_FIELD_QX_PREV 5  /*   before the last step, except cells the step does not write */
+#define FIP_FIELD_QY_PREV 6
+#define FIP_FIELD_TERRAIN 7  /* d_sohle */
+#define FIP_FIELD_Z 8        /* water level h + terrain */
+
+typedef struct fip_handle fip_handle;
+
+typedef struct {
+  int device;               /* CUDA device ordinal (default 0) */
+  int use_graphs;           /* run batches of steps as captured CUDA graphs (default 1) */
+  int all_tiles;            /* compute every tile every step, no dry-tile skipping (default 0) */
+  int stop_on_nonfinite;    /* fip_step/fip_run return FIP_ERR_NONFINITE at the first NaN/Inf depth */
+  int quiet;                /* write no sampling CSV (default 0: stdout, like the reference) */
+  const char* sample_path;  /* write the sampling CSV to this file instead of stdout (NULL) */
+} fip_options;
+
+typedef struct {
+  int W, H;
+  int pitch;                /* device row pitch in elements (cudaMallocPitch, like the reference) */
+  int n_tiles;              /* 480 x 32-cell tiles of the domain */
+  int active_tiles;         /* tiles computed by the next step */
+  int iteration;
+  double duration;
+  float dt;
+  float last_cfl;           /* CFL minimum of the last step (<= 1) */
+  int nonfinite;            /* a stored depth has been NaN/Inf */
+} fip_info_t;
+
+void fip_default_options(fip_options* opt);
+
+/* SimData::loadSimData + initDeviceBuffers (src/simdata.cpp:238-310, :54-96) and
+ * BoundaryConditionKernel::generate (src/bc_kernel_gen.cpp:154-192); also prints the sampling
+ * header like main() (src/main.cpp:225-226). */
+int fip_init(const char* yaml_path, fip_handle** out);
+int fip_init_ex(const char* yaml_path, const fip_options* opt, fip_handle** out);
+
+/* n_steps calls of simulate() (src/main.cpp:100-135): dt control, sampling, compute kernel
+ * (launchComputeKernel, src/kernels.cu:441-455), boundary conditions
+ * (launchBoundaryConditionKernel, src/main.cpp:85-98), flood plains every 100 iterations
+ * (launchFloodPlainKernel, src/kernels.cu:457-463) and save_state dumps. */
+int fip_step(fip_handle* h, int n_steps);
+
+/* The headless loop of main(): while (duration < target_duration) simulate();
+ * (src/main.cpp:243-246). */
+int fip_run(fip_handle* h);
+
+/* dumpDeviceBuffers (src/main.cpp:180-202): <prefix>_{ah,qx,qy,flood_plains}_<int(duration)>_<UTC
+ * %Y-%m-%d-%H-%M>, each 2 x size_t (W, H) + W*H float32, of the buffers the reference dumps (the
+ * ping-pong partners, i.e. the state before the last step) and hmax. prefix NULL = the YAML name. */
+int fip_save(fip_handle* h, const char* prefix_or_null);
+
+/* Same file format, of the current state (d_h1, d_qx1, d_qy1) and hmax; no counterpart in the
+ * reference (its dumps always hold the state before the last step). */
+int fip_save_current(fip_handle* h, const char* prefix_or_null);
+
+/* sample (src/main.cpp:53-83): one "duration;v1;v2;...;" row of the configured points now. */
+int fip_sample(fip_handle* h);
+
+/* FP64 volume sum(h) * dx^2 of the current state (the commented-out volume check of
+ * src/main.cpp:139-149, on the device). */
+int fip_volume(fip_handle* h, double* out);
+
+/* Copies one field (FIP_FIELD_*) into a caller-provided host buffer of W*H floats
+ * (dumpDeviceBuffer, src/main.cpp:170-178). */
+int fip_get_field(fip_handle* h, int field, float* host_out);
+
+/* duration (s, FP64), dt of the next step, completed iterations (SimData::duration/dt/iteration). */
+int fip_time(fip_handle* h, double* duration, float* dt, int* iteration);
+
+int fip_info(fip_handle* h, fip_info_t* out);
+
+/* Device time of the two kernels of a step, measured with CUDA events around each launch of
+ * n_steps eager (not graph) steps: average ms per launch. No counterpart in the reference. */
+int fip_profile_steps(fip_handle* h, int n_steps, float* stencil_ms, float* post_ms);
+
+/* Frees every device and host resource of the handle (the reference leaves this to
+ * cudaDeviceReset at exit, src/main.cpp:256). */
+void fip_destroy(fip_handle* h);
+
+/* ---- host-only entry points (no GPU needed) ---- */
+
+/* Parses and validates a parameter file and loads its grids, without touching a GPU
+ * (validateSimDataConfig + loadSimData, src/simdata.cpp:152-310). Messages as fip_init. */
+int fip_validate(const char* yaml_path);
+
+/* The parsed configuration as a JSON object (name, W, H, dx, dt, variable_dt, solver,
+ * target_duration, kSt, no_data, kst_var, boundary_conditions, sampling, save_state), written
+ * to buf (NUL-terminated, truncated to buflen). Returns the full length or a negative error. */
+int fip_config_json(const char* yaml_path, char* buf, int buflen);
+
+/* CUDA source of the boundary-condition program for a parameter file and a device row pitch in
+ * elements (BoundaryConditionKernel::generate's source text, src/bc_kernel_gen.cpp:154-178).
+ * When compile != 0 it is also compiled with NVRTC for sm_100a (no GPU needed). Returns the
+ * source length or a negative error. */
+int fip_bc_program(const char* yaml_path, int pitch, int compile, char* buf, int buflen);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* fip_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
