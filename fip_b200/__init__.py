@@ -58,10 +58,17 @@ class Simulation:
         _lib.check(_lib.lib().fip_sample(self._h))
 
     # -- state -----------------------------------------------------------------------------
-    def field(self, name: str = "h") -> np.ndarray:
-        out = np.empty((self.H, self.W), np.float32)
+    def field(self, name: str = "h", out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.H, self.W), np.float32)
+        assert out.dtype == np.float32 and out.shape == (self.H, self.W) and out.flags.c_contiguous
         _lib.check(_lib.lib().fip_get_field(self._h, FIELDS[name], out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
+
+    def set_field(self, name: str, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float32)
+        assert a.shape == (self.H, self.W)
+        _lib.check(_lib.lib().fip_set_field(self._h, FIELDS[name], a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
 
     def volume(self) -> float:
         v = ctypes.c_double()
@@ -91,6 +98,12 @@ class Simulation:
         a, b = ctypes.c_float(), ctypes.c_float()
         _lib.check(_lib.lib().fip_profile_steps(self._h, int(n), ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def step_timed(self, n: int):
+        """n steps in one graph, timed on the device: (total ms, stencil ms/launch, post ms/launch)."""
+        t, a, b = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        _lib.check(_lib.lib().fip_step_timed(self._h, int(n), ctypes.byref(t), ctypes.byref(a), ctypes.byref(b)))
+        return t.value, a.value, b.value
 
     # -- lifetime --------------------------------------------------------------------------
     def close(self) -> None:

@@ -144,8 +144,10 @@ extern "C" __global__ void __launch_bounds__(FIP_POST_THREADS) fip_post(const Fi
   FipCtl* ctl = a.ctl;
   if (*((volatile int*)&ctl->stop)) return;
   const bool step_mode = (a.mode == FIP_POST_MODE_STEP);
-  const int k = step_mode ? ctl->iteration : -1;
+  // the plan is for the step after k: the coming step in INIT/PLAN mode
+  const int k = step_mode ? ctl->iteration : ctl->iteration - 1;
   if (blockIdx.x == 0) {
+    if (a.mode == FIP_POST_MODE_PLAN) return;
     const int cur = step_mode ? (ctl->parity ^ 1) : ctl->parity;
     const double t_d = step_mode ? ctl->duration + (double)ctl->dt : ctl->duration;
     const float t = __double2float_rn(t_d);  // TimeSeries::interp(float time)

@@ -59,6 +59,7 @@ struct FipCtl {
 
 #define FIP_POST_MODE_STEP 0   // after a step: BCs at duration+dt, plan, advance the control block
 #define FIP_POST_MODE_INIT 1   // before the first step: BCs at duration, plan from the initial state
+#define FIP_POST_MODE_PLAN 2   // plan from the current state only (after the host replaced a field)
 
 // Argument block of the generated post kernel (passed by value; same layout on both sides).
 struct FipPostArgs {

@@ -775,8 +775,8 @@ cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t strea
   return st.kst ? launch_step_t<true>(st, grid, stream) : launch_step_t<false>(st, grid, stream);
 }
 
-cudaError_t launch_init_tiles(const StencilState& st, cudaStream_t stream) {
-  init_tiles_kernel<<<st.n_tiles, 256, 0, stream>>>(st.h[0], st.qx[0], st.qy[0], st.sohle, st.W, st.H, st.pitch,
+cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t stream) {
+  init_tiles_kernel<<<st.n_tiles, 256, 0, stream>>>(st.h[parity], st.qx[parity], st.qy[parity], st.sohle, st.W, st.H, st.pitch,
                                                     st.no_value, st.n_ty, st.n_tiles, st.sticky, st.nz[0], st.nz[1]);
   return cudaGetLastError();
 }

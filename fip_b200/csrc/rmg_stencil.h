@@ -37,8 +37,8 @@ int make_tensor_maps(StencilState* st);
 // One rmg step over the active tiles of the current plan (reads ctl on the device).
 cudaError_t launch_rmg_step(const StencilState& st, int grid_ctas, cudaStream_t stream);
 
-// Per-tile sticky flags and the nonzero flags of the initial state (both parities).
-cudaError_t launch_init_tiles(const StencilState& st, cudaStream_t stream);
+// Per-tile sticky flags and the nonzero flags of state buffer `parity` (into both nz slots).
+cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t stream);
 
 // hmax = max(hmax, h[parity]) over the whole grid (the reference's flood_plains_kernel).
 cudaError_t launch_hmax_fold(const StencilState& st, int parity, cudaStream_t stream);

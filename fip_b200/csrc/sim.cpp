@@ -73,6 +73,7 @@ struct fip_handle {
   float* h_sample_val = nullptr;
   int grid_ctas = 0;
   bool started = false;     // the iteration-0 boundary conditions have run
+  bool replan = false;      // the host replaced state fields: recompute the active tiles
   double sample_timer = 0;  // Sampling::timer
   size_t save_pos = 0;
   std::map<int, cudaGraphExec_t> graphs;
@@ -231,7 +232,7 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
     h_ctl->dt = d;
   }
   ck(cudaMemcpy(d_ctl, h_ctl, sizeof(FipCtl), cudaMemcpyHostToDevice), "cudaMemcpy");
-  ck(fip::launch_init_tiles(st, stream), "init_tiles");
+  ck(fip::launch_init_tiles(st, 0, stream), "init_tiles");
   grid_ctas = fip::rmg_step_grid(device);
 
   // boundary-condition program (BoundaryConditionKernel::generate)
@@ -419,6 +420,11 @@ int fip_handle::run_steps(long long budget, bool to_target) {
     launch_post(FIP_POST_MODE_INIT);
     started = true;
   }
+  if (replan) {
+    ck(fip::launch_init_tiles(st, h_ctl->parity, stream), "init_tiles");
+    launch_post(FIP_POST_MODE_PLAN);
+    replan = false;
+  }
   h_ctl->target = to_target ? cfg.target_duration : kInf;
   h_ctl->steps_left = budget > (1LL << 30) ? (1 << 30) : (int)budget;
   h_ctl->stop = 0;
@@ -589,6 +595,34 @@ int fip_get_field(fip_handle* h, int field, float* dst) {
   });
 }
 
+int fip_set_field(fip_handle* h, int field, const float* src) {
+  if (!h || !src) return fail(FIP_ERR_ARG, "null argument");
+  if (field != FIP_FIELD_H && field != FIP_FIELD_QX && field != FIP_FIELD_QY)
+    return fail(FIP_ERR_ARG, "fip_set_field: only FIP_FIELD_H, FIP_FIELD_QX and FIP_FIELD_QY can be set");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    const int p = h->h_ctl->parity;
+    float* const* bufs = field == FIP_FIELD_H ? h->st.h : field == FIP_FIELD_QX ? h->st.qx : h->st.qy;
+    const size_t W = h->cfg.W, H = h->cfg.H, pb = (size_t)h->st.pitch * 4;
+    ck(cudaMemcpy2DAsync(bufs[p], pb, src, W * 4, W * 4, H, cudaMemcpyHostToDevice, h->stream), "fip_set_field");
+    ck(cudaMemcpy2DAsync(bufs[p ^ 1], pb, bufs[p], pb, W * 4, H, cudaMemcpyDeviceToDevice, h->stream),
+       "fip_set_field");
+    if (field == FIP_FIELD_H && !h->h_ctl->hmax_full) {
+      bool negative = false;
+      for (size_t i = 0; i < W * H && !negative; ++i) negative = src[i] < 0.f;
+      if (negative) {
+        h->h_ctl->hmax_full = 1;
+        ck(cudaMemcpyAsync(&h->d_ctl->hmax_full, &h->h_ctl->hmax_full, sizeof(int), cudaMemcpyHostToDevice,
+                           h->stream),
+           "fip_set_field");
+      }
+    }
+    h->replan = true;
+    ck(cudaStreamSynchronize(h->stream), "fip_set_field");
+    return FIP_OK;
+  });
+}
+
 int fip_time(fip_handle* h, double* duration, float* dt, int* iteration) {
   if (!h) return fail(FIP_ERR_ARG, "null handle");
   if (duration) *duration = h->h_ctl->duration;
@@ -667,6 +701,73 @@ int fip_profile_steps(fip_handle* h, int n, float* stencil_ms, float* post_ms) {
     h->h_ctl->stop_reason = 0;
     h->write_ctl_fields();
     ck(cudaStreamSynchronize(h->stream), "profile");
+    return FIP_OK;
+  });
+}
+
+int fip_step_timed(fip_handle* h, int n, float* total_ms, float* stencil_ms, float* post_ms) {
+  if (!h || n <= 0) return fail(FIP_ERR_ARG, "bad argument");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    if (!h->started) {
+      int rc = h->run_steps(1, false);
+      if (rc) return rc;
+    }
+    if (h->replan) {
+      ck(fip::launch_init_tiles(h->st, h->h_ctl->parity, h->stream), "init_tiles");
+      h->launch_post(FIP_POST_MODE_PLAN);
+      h->replan = false;
+    }
+    const double keep_sample = h->h_ctl->next_sample, keep_save = h->h_ctl->next_save;
+    h->h_ctl->next_sample = kInf;
+    h->h_ctl->next_save = kInf;
+    h->h_ctl->target = kInf;
+    h->h_ctl->steps_left = n;
+    h->h_ctl->stop = 0;
+    h->h_ctl->stop_reason = 0;
+    h->write_ctl_fields();
+    std::vector<cudaEvent_t> ev(2 * n + 1);
+    for (auto& e : ev) ck(cudaEventCreate(&e), "event");
+    cudaGraph_t g;  // event record nodes (cudaEventRecordExternal) timestamp every launch
+    ck(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "capture");
+    for (int i = 0; i < n; ++i) {
+      ck(cudaEventRecordWithFlags(ev[2 * i], h->stream, cudaEventRecordExternal), "event");
+      ck(fip::launch_rmg_step(h->st, h->grid_ctas, h->stream), "rmg_step");
+      ck(cudaEventRecordWithFlags(ev[2 * i + 1], h->stream, cudaEventRecordExternal), "event");
+      h->launch_post(FIP_POST_MODE_STEP);
+    }
+    ck(cudaEventRecordWithFlags(ev[2 * n], h->stream, cudaEventRecordExternal), "event");
+    ck(cudaStreamEndCapture(h->stream, &g), "capture");
+    cudaGraphExec_t ex;
+    ck(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate");
+    cudaGraphDestroy(g);
+    ck(cudaGraphUpload(ex, h->stream), "cudaGraphUpload");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    ck(cudaGraphLaunch(ex, h->stream), "cudaGraphLaunch");
+    h->read_ctl();
+    double tot = 0, s = 0, p = 0;
+    float x = 0;
+    ck(cudaEventElapsedTime(&x, ev[0], ev[2 * n]), "event");
+    tot = x;
+    for (int i = 0; i < n; ++i) {
+      ck(cudaEventElapsedTime(&x, ev[2 * i], ev[2 * i + 1]), "event");
+      s += x;
+      ck(cudaEventElapsedTime(&x, ev[2 * i + 1], ev[2 * i + 2]), "event");
+      p += x;
+    }
+    cudaGraphExecDestroy(ex);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (total_ms) *total_ms = (float)tot;
+    if (stencil_ms) *stencil_ms = (float)(s / n);
+    if (post_ms) *post_ms = (float)(p / n);
+    const int err = h->h_ctl->error;
+    h->h_ctl->next_sample = keep_sample;
+    h->h_ctl->next_save = keep_save;
+    h->h_ctl->stop = 0;
+    h->h_ctl->stop_reason = 0;
+    h->write_ctl_fields();
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    if (err) return fail(FIP_ERR_DEVICE_TIMEOUT, "device wait ran out (code " + std::to_string(err) + ")");
     return FIP_OK;
   });
 }

@@ -101,6 +101,13 @@ int fip_volume(fip_handle* h, double* out);
  * (dumpDeviceBuffer, src/main.cpp:170-178). */
 int fip_get_field(fip_handle* h, int field, float* host_out);
 
+/* Replaces one field of the current state (FIP_FIELD_H, _QX or _QY) from a host buffer of W*H
+ * floats, in both ping-pong buffers like initDeviceBuffers does for the initial state
+ * (src/simdata.cpp:82-88); the active tiles are re-planned before the next step. Pinned host
+ * memory makes the copy asynchronous-fast. No counterpart in the reference (which restarts only
+ * from files at start-up). */
+int fip_set_field(fip_handle* h, int field, const float* host_src);
+
 /* duration (s, FP64), dt of the next step, completed iterations (SimData::duration/dt/iteration). */
 int fip_time(fip_handle* h, double* duration, float* dt, int* iteration);
 
@@ -109,6 +116,12 @@ int fip_info(fip_handle* h, fip_info_t* out);
 /* Device time of the two kernels of a step, measured with CUDA events around each launch of
  * n_steps eager (not graph) steps: average ms per launch. No counterpart in the reference. */
 int fip_profile_steps(fip_handle* h, int n_steps, float* stencil_ms, float* post_ms);
+
+/* n_steps steps as one CUDA graph with an event record around every stencil launch, timed on
+ * the handle's stream: total device ms of the n steps and the average ms per launch of the
+ * stencil and post kernels. Sampling, dumps and the target duration are not checked during
+ * these steps (the state advances normally otherwise). No counterpart in the reference. */
+int fip_step_timed(fip_handle* h, int n_steps, float* total_ms, float* stencil_ms, float* post_ms);
 
 /* Frees every device and host resource of the handle (the reference leaves this to
  * cudaDeviceReset at exit, src/main.cpp:256). */
