@@ -76,8 +76,12 @@ class Clocks:
                                        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            t0 = time.time()  # keep nvidia-smi's start-up out of the timed region
+            while not self.samples and time.time() - t0 < 10:
+                time.sleep(0.05)
         except Exception:
             self._p = None
+        self.first = len(self.samples)
         return self
 
     def _read(self):
@@ -87,6 +91,7 @@ class Clocks:
                 self.samples.append(parts)
 
     def __exit__(self, *exc):
+        self.last = len(self.samples)
         if self._p:
             self._p.terminate()
             try:
@@ -95,14 +100,15 @@ class Clocks:
                 self._p.kill()
 
     def summary(self):
-        if not self.samples:
+        during = self.samples[max(0, self.first - 1):max(self.last, self.first)]
+        if not during:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        sm = [float(s[1]) for s in during if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in during if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i].lower() == "active"})
+        reasons = sorted({names[i] for s in during for i in range(4) if s[4 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(during)}
 
 
 def make_workload(args, rank):
