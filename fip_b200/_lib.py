@@ -25,7 +25,7 @@ FIELDS = {"h": 0, "qx": 1, "qy": 2, "hmax": 3, "h_prev": 4, "qx_prev": 5, "qy_pr
 
 # every symbol include/fip.h declares
 EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_run", "fip_save", "fip_save_current",
-           "fip_sample", "fip_volume", "fip_get_field", "fip_set_field", "fip_time", "fip_info", "fip_profile_steps", "fip_step_timed", "fip_destroy",
+           "fip_sample", "fip_volume", "fip_get_field", "fip_set_field", "fip_time", "fip_info", "fip_profile_steps", "fip_step_timed", "fip_destroy", "fip_rmg_step_noalloc",
            "fip_last_error", "fip_validate", "fip_config_json", "fip_bc_program")
 
 
@@ -74,6 +74,9 @@ def lib():
         L.fip_info.argtypes = [vp, ctypes.POINTER(FipInfo)]
         L.fip_profile_steps.argtypes = [vp, ip, fp, fp]
         L.fip_step_timed.argtypes = [vp, ip, fp, fp, fp]
+        L.fip_rmg_step_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_float, vp, vp, vp, ip, ip, ip, ctypes.c_float,
+                                           ctypes.c_float, ctypes.c_float, vp, vp]
+        L.fip_rmg_step_noalloc.restype = ctypes.c_int
         L.fip_destroy.argtypes = [vp]
         L.fip_destroy.restype = None
         L.fip_last_error.restype = ctypes.c_char_p

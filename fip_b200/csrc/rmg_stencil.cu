@@ -23,6 +23,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <string>
+
 #include "drv.h"
 #include "fip_ctl.h"
 #include "rmg_stencil.h"
@@ -803,4 +806,162 @@ cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, cons
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------------------------
+// One rmg step without any device allocation (fip_rmg_step_noalloc in include/fip.h).
+//
+// Some callers cannot allocate device memory: a host that drives this step from its own time
+// loop while other streams keep the GPU busy (cudaFree synchronises the whole device), a host
+// that owns all device memory through its own pool and forbids allocations once it runs, or
+// code that records the step into a CUDA graph. For them the step's scratch (control block,
+// tile list, per-tile wet flags) lives in the file-scope array below, which every GPU that loads
+// the library holds until the process exits. It holds the plan of at most kNoAllocMaxTiles tiles
+// of 480 x 32 cells (about 503 million cells); larger grids are rejected. All calls share it and
+// it keeps the last call's contents, so each call first rewrites everything the step reads from
+// it; calls that overlap on the GPU (several streams, several host threads) race on it.
+namespace {
+
+constexpr int kNoAllocMaxTiles = 32768;
+constexpr int kNoAllocMaxChunks = kNoAllocMaxTiles / FIP_PLAN_CHUNK;
+constexpr size_t kNoAllocCtlOff = 0;
+constexpr size_t kNoAllocCntOff = 256;
+constexpr size_t kNoAllocListOff = kNoAllocCntOff + sizeof(int) * kNoAllocMaxChunks;
+constexpr size_t kNoAllocNzOff = kNoAllocListOff + sizeof(int) * kNoAllocMaxTiles;
+constexpr size_t kNoAllocBytes = kNoAllocNzOff + kNoAllocMaxTiles;
+static_assert(sizeof(FipCtl) <= kNoAllocCntOff, "control block must fit its slot");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Rewrites the part of the scratch the step reads: the control block (dt, a fresh CFL minimum,
+// no fold, no stop) and the identity plan over all n_tiles tiles.
+__global__ void noalloc_setup_kernel(unsigned char* scratch, float dt, int n_tiles, int n_chunks) {
+  FipCtl* ctl = reinterpret_cast<FipCtl*>(scratch + kNoAllocCtlOff);
+  int* cnt = reinterpret_cast<int*>(scratch + kNoAllocCntOff);
+  int* list = reinterpret_cast<int*>(scratch + kNoAllocListOff);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid == 0) {
+    ctl->duration = 0.0;
+    ctl->next_sample = ctl->next_save = ctl->target = 0.0;
+    ctl->dt = dt;
+    ctl->last_cfl = 1.0f;
+    ctl->iteration = 0;
+    ctl->parity = 0;
+    ctl->stop = 0;
+    ctl->stop_reason = 0;
+    ctl->steps_left = 0;
+    ctl->variable_dt = 0;
+    ctl->stop_on_nonfinite = 0;
+    ctl->nonfinite = 0;
+    ctl->error = 0;
+    ctl->hmax_every = 0;
+    ctl->hmax_full = 0;
+    ctl->force_all = 1;
+    ctl->cfl_bits[0] = ctl->cfl_bits[1] = __float_as_uint(1.0f);
+    ctl->post_done = 0u;
+  }
+  for (int c = tid; c < n_chunks; c += gridDim.x * blockDim.x)
+    cnt[c] = min(FIP_PLAN_CHUNK, n_tiles - c * FIP_PLAN_CHUNK);
+  for (int t = tid; t < n_tiles; t += gridDim.x * blockDim.x) list[t] = t;
+}
+
+// CFL minimum of the step (NaN when a device-side wait ran out).
+__global__ void noalloc_finish_kernel(const unsigned char* scratch, float* cfl_out) {
+  const FipCtl* ctl = reinterpret_cast<const FipCtl*>(scratch + kNoAllocCtlOff);
+  *cfl_out = ctl->error ? __int_as_float(0x7fc00000) : __uint_as_float(ctl->cfl_bits[0]);
+}
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+// Device address of the scratch on the current device; cudaGetSymbolAddress once per device.
+cudaError_t noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
+  return cudaSuccess;
+}
+
+}  // namespace
+
+void set_last_error(const std::string& msg);
+
 }  // namespace fip
+
+extern "C" int fip_rmg_step_noalloc(const float* h_in, const float* qx_in, const float* qy_in, const float* terrain,
+                                    const float* kst_or_null, float kst_fixed, float* h_out, float* qx_out,
+                                    float* qy_out, int W, int H, int pitch, float dx, float dt, float no_value,
+                                    float* cfl_out_or_null, void* stream) {
+  using namespace fip;
+  auto bad = [](int code, const std::string& m) {
+    set_last_error(m);
+    return code;
+  };
+  if (W < 4 || H < 4) return bad(-7, "fip_rmg_step_noalloc: the grid must be at least 4 x 4 cells");
+  if (pitch < W || (pitch % 4) != 0)
+    return bad(-7, "fip_rmg_step_noalloc: pitch must be >= W and a multiple of 4 elements (16 bytes)");
+  int n_sx, n_ty, n_tiles, n_chunks;
+  tile_geometry(W, H, &n_sx, &n_ty, &n_tiles, &n_chunks);
+  if (n_tiles > kNoAllocMaxTiles)
+    return bad(-7, "fip_rmg_step_noalloc: a " + std::to_string(W) + " x " + std::to_string(H) + " grid has " +
+                       std::to_string(n_tiles) + " tiles of 480 x 32 cells; the static scratch holds at most " +
+                       std::to_string(kNoAllocMaxTiles));
+  const void* ptrs[] = {h_in, qx_in, qy_in, terrain, h_out, qx_out, qy_out};
+  for (const void* p : ptrs)
+    if (!p || (reinterpret_cast<uintptr_t>(p) & 15u))
+      return bad(-7, "fip_rmg_step_noalloc: every field must be a non-null, 16-byte aligned device pointer");
+  if (kst_or_null && (reinterpret_cast<uintptr_t>(kst_or_null) & 15u))
+    return bad(-7, "fip_rmg_step_noalloc: kSt grid must be 16-byte aligned");
+  if (!(dt > 0.f) || !(dx > 0.f)) return bad(-7, "fip_rmg_step_noalloc: dt and dx must be positive");
+  std::string derr;
+  if (!drv::load(&derr)) return bad(-3, derr);
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  unsigned char* scratch = nullptr;
+  if (e == cudaSuccess) e = noalloc_scratch(device, &scratch);
+  if (e != cudaSuccess) return bad(-3, std::string("fip_rmg_step_noalloc: scratch address: ") + cudaGetErrorString(e));
+
+  StencilState st{};
+  st.h[0] = const_cast<float*>(h_in);
+  st.h[1] = h_out;
+  st.qx[0] = const_cast<float*>(qx_in);
+  st.qx[1] = qx_out;
+  st.qy[0] = const_cast<float*>(qy_in);
+  st.qy[1] = qy_out;
+  st.sohle = const_cast<float*>(terrain);
+  st.kst = const_cast<float*>(kst_or_null);
+  st.hmax = nullptr;
+  st.ctl = reinterpret_cast<FipCtl*>(scratch + kNoAllocCtlOff);
+  st.sticky = nullptr;
+  for (int b = 0; b < 2; ++b) {
+    st.nz[b] = scratch + kNoAllocNzOff;
+    st.list[b] = reinterpret_cast<int*>(scratch + kNoAllocListOff);
+    st.chunk_cnt[b] = reinterpret_cast<int*>(scratch + kNoAllocCntOff);
+  }
+  st.W = W;
+  st.H = H;
+  st.pitch = pitch;
+  st.n_sx = n_sx;
+  st.n_ty = n_ty;
+  st.n_tiles = n_tiles;
+  st.n_chunks = n_chunks;
+  st.dx = dx;
+  st.kst_fixed = kst_fixed;
+  st.no_value = no_value;
+  const int tr = make_tensor_maps(&st);
+  if (tr) return bad(-3, drv::message((CUresult)tr, "fip_rmg_step_noalloc: cuTensorMapEncodeTiled"));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  noalloc_setup_kernel<<<(n_tiles + 255) / 256, 256, 0, s>>>(scratch, dt, n_tiles, n_chunks);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = launch_rmg_step(st, rmg_step_grid(device), s);
+  if (e == cudaSuccess && cfl_out_or_null) {
+    noalloc_finish_kernel<<<1, 1, 0, s>>>(scratch, cfl_out_or_null);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) return bad(-3, std::string("fip_rmg_step_noalloc: ") + cudaGetErrorString(e));
+  return 0;
+}

@@ -55,6 +55,10 @@ constexpr double kInf = std::numeric_limits<double>::infinity();
 
 }  // namespace
 
+namespace fip {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace fip
+
 struct fip_handle {
   fip::Config cfg;
   fip_options opt;

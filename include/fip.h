@@ -127,6 +127,31 @@ int fip_step_timed(fip_handle* h, int n_steps, float* total_ms, float* stencil_m
  * cudaDeviceReset at exit, src/main.cpp:256). */
 void fip_destroy(fip_handle* h);
 
+/* One rmg step of the whole grid on caller-owned device buffers, allocating nothing. No
+ * counterpart in the reference. It is for callers that cannot allocate device memory: a host that
+ * drives the step from its own time loop while other streams keep the GPU busy (cudaFree
+ * synchronises the whole device), a host whose own pool owns all device memory, or code that
+ * records the step into a CUDA graph.
+ * Inputs: h_in, qx_in, qy_in, terrain (and kst_or_null, else the uniform kst_fixed), pitched with
+ * `pitch` elements per row (a multiple of 4), 16-byte aligned, W x H cells, W, H >= 4. Outputs:
+ * h_out, qx_out, qy_out receive the step on the cells the reference's kernel writes; their other
+ * cells are left as the caller set them (give them the input state, like the reference's
+ * ping-pong partner). cfl_out_or_null (device float) receives the CFL minimum of the step (NaN if
+ * a bounded device-side wait ran out). No boundary conditions, dt control or sampling: this is the
+ * stencil alone (the launch of src/kernels.cu:441-455 with the mask off).
+ * Scratch: a static device array sized for grids of at most 32768 tiles of 480 x 32 cells (about
+ * 503 million cells); larger grids return FIP_ERR_ARG. Every GPU that loads the library holds
+ * that array (about 160 KB) until the process exits. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture. Calls share the array and overwrite what the step reads from it each time; calls that
+ * overlap on the GPU (other streams or host threads) race on it. Runs on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream) on the current device and returns without
+ * synchronising. */
+int fip_rmg_step_noalloc(const float* h_in, const float* qx_in, const float* qy_in, const float* terrain,
+                         const float* kst_or_null, float kst_fixed, float* h_out, float* qx_out, float* qy_out,
+                         int W, int H, int pitch, float dx, float dt, float no_value, float* cfl_out_or_null,
+                         void* stream);
+
 /* ---- host-only entry points (no GPU needed) ---- */
 
 /* Parses and validates a parameter file and loads its grids, without touching a GPU
