@@ -37,7 +37,17 @@ namespace {
 constexpr float kDH = 0.01f;         // src/kernels.cu:23
 constexpr float kEPS = 10e-7f;       // src/kernels.cu:24 (EPS_TROCKEN)
 constexpr float kG = 9.81f;          // src/simdata.h:358
-constexpr int kNSlot = 8;            // ring depth in rows
+#ifndef FIP_NSLOT_KVAR
+#define FIP_NSLOT_KVAR 7
+#endif
+#ifndef FIP_NSLOT_UNIFORM
+#define FIP_NSLOT_UNIFORM 8
+#endif
+constexpr int kNSlotMax = 8;  // ring depth in rows: 7 with the kSt field (3 CTAs per SM fit), else 8
+#ifndef FIP_MIN_CTAS
+#define FIP_MIN_CTAS 3
+#endif
+constexpr int kMinCtas = FIP_MIN_CTAS;  // resident CTAs per SM
 constexpr int kFieldBytes = FIP_SMEM_COLS * 4;  // 2048 B per staged row of one field
 constexpr int kConsumerWarps = 4;
 constexpr int kThreads = (kConsumerWarps + 1) * 32;
@@ -110,49 +120,47 @@ __device__ __forceinline__ void record_error(FipCtl* ctl, int code) { atomicCAS(
 // fp32div_wrapper (src/kernels.cu:30-33)
 __device__ __forceinline__ float fdivw(float a, float b) { return (a == 0.0f) ? 0.0f : (a / b); }
 
-// compute_rmg_qx (src/kernels.cu:75-100); same operand order, so the same rounding
-__device__ __forceinline__ float upd_qx(float fx_east, float fx_i, float gx_i, float gx_south, float dt, float dx,
-                                        float dt_inv, float dx_inv, float kst, float h_i, float h_east,
-                                        float s_east, float s_i, float qx_i, float qy_i, float qy_e, float qy_s,
-                                        float qy_se) {
+// compute_rmg_qx / compute_rmg_qy (src/kernels.cu:75-127), split in two so that a warp can
+// skip the friction factor when none of its cells moves (the reference selects 0 there):
+//   mom_depth: a0 = max(0, mean depth of the face), a1 = max(a0, DH)
+//   friction : dt * G / (kSt * kSt) * sqrt(ux^2 + uy^2) * (1 / a1)^2.33, the caller selects 0
+//              when ux == 0 && uy == 0 (discharges, not velocities, :91-94)
+//   upd_q*   : the rest, same operand order as the reference so the same rounding.
+// lim_i = h_i * dt_inv * dx * 0.25f comes precomputed per cell; the east (north) clamp
+// -h_east * dt_inv * dx * 0.25f equals -lim of the east (north) cell exactly, since a negation
+// commutes with rounding.
+__device__ __forceinline__ float friction(float fric, float ux, float uy, float a1) {
+  const float inv = 1.f / a1;
+  return fric * sqrtf(ux * ux + uy * uy) * powf(inv, 2.33f);
+}
+
+__device__ __forceinline__ float upd_qx(float fx_east, float fx_i, float gx_i, float gx_south, float dt, float dx_inv,
+                                        float reib, float a0, float h_i, float h_east, float s_east, float s_i,
+                                        float qx_i, float lim_i, float lim_e) {
   float dfx = (fx_east - fx_i) * dx_inv;
   float dgx = (gx_i - gx_south) * dx_inv;
-  float a = (h_i + h_east) * .5f;
-  a = fmaxf(0.f, a);
-  float dhg = a * kG * (-s_east + s_i) * dx_inv;
+  float dhg = a0 * kG * (-s_east + s_i) * dx_inv;
   float dhx = (0.5f * kG * h_east * h_east - 0.5f * kG * h_i * h_i) * dx_inv;
-  a = fmaxf(a, kDH);
-  const float inv = 1.f / a;
-  const float ux = qx_i;
-  const float uy = (qy_i + qy_e + qy_s + qy_se) * 0.25f;
-  float reib = ((ux == 0.f) && (uy == 0.f)) ? 0.f : (dt * kG / (kst * kst) * sqrtf(ux * ux + uy * uy) * powf(inv, 2.33f));
   float q = fdivw(qx_i + dt * (-dfx - dgx - dhx + dhg), (1.f + reib));
-  q = fminf(q, h_i * dt_inv * dx * 0.25f);
-  q = fmaxf(q, -h_east * dt_inv * dx * 0.25f);
+  q = fminf(q, lim_i);
+  q = fmaxf(q, -lim_e);
   return q;
 }
 
-// compute_rmg_qy (src/kernels.cu:102-127)
-__device__ __forceinline__ float upd_qy(float fy_i, float fy_west, float gy_i, float gy_north, float dt, float dx,
-                                        float dt_inv, float dx_inv, float kst, float h_i, float h_north,
-                                        float s_north, float s_i, float qy_i, float qx_i, float qx_w, float qx_n,
-                                        float qx_nw) {
+__device__ __forceinline__ float upd_qy(float fy_i, float fy_west, float gy_i, float gy_north, float dt, float dx_inv,
+                                        float reib, float a0, float h_i, float h_north, float s_north, float s_i,
+                                        float qy_i, float lim_i, float lim_n) {
   float dgy = (gy_north - gy_i) * dx_inv;
   float dfy = (fy_i - fy_west) * dx_inv;
-  float a = (h_i + h_north) * .5f;
-  a = fmaxf(0.f, a);
-  float dhg = a * kG * (s_i - s_north) * dx_inv;
+  float dhg = a0 * kG * (s_i - s_north) * dx_inv;
   float dhy = (0.5f * kG * h_north * h_north - 0.5f * kG * h_i * h_i) * dx_inv;
-  a = fmaxf(a, kDH);
-  float inv = 1.f / a;
-  float ux = (qx_i + qx_n + qx_w + qx_nw) * 0.25f;
-  float uy = qy_i;
-  float reib = ((ux == 0.f) && (uy == 0.f)) ? 0.f : (dt * kG / (kst * kst) * sqrtf(ux * ux + uy * uy) * powf(inv, 2.33f));
   float q = fdivw(qy_i + dt * (-dgy - dfy - dhy + dhg), (1 + reib));
-  q = fminf(q, h_i * dt_inv * dx * 0.25f);
-  q = fmaxf(q, -h_north * dt_inv * dx * 0.25f);
+  q = fminf(q, lim_i);
+  q = fmaxf(q, -lim_n);
   return q;
 }
+
+__device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
 
 __device__ __forceinline__ float4 lds4(const unsigned char* slot, int field, int col) {
   return *reinterpret_cast<const float4*>(slot + field * kFieldBytes + col * 4);
@@ -201,17 +209,18 @@ __device__ __forceinline__ bool next_run(Walk& w, const int* list, const int* s_
 }
 
 template <bool KVAR>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, kMinCtas)
     rmg_step_kernel(const __grid_constant__ CUtensorMap tm_h0, const __grid_constant__ CUtensorMap tm_h1,
                     const __grid_constant__ CUtensorMap tm_qx0, const __grid_constant__ CUtensorMap tm_qx1,
                     const __grid_constant__ CUtensorMap tm_qy0, const __grid_constant__ CUtensorMap tm_qy1,
                     const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_k,
                     const StepArgs a) {
   constexpr int NF = KVAR ? 5 : 4;
+  constexpr int kNSlot = KVAR ? FIP_NSLOT_KVAR : FIP_NSLOT_UNIFORM;
   constexpr int kSlotBytes = NF * kFieldBytes;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
-  __shared__ __align__(8) uint64_t full_bar[kNSlot];
-  __shared__ __align__(8) uint64_t empty_bar[kNSlot];
+  __shared__ __align__(8) uint64_t full_bar[kNSlotMax];
+  __shared__ __align__(8) uint64_t empty_bar[kNSlotMax];
   __shared__ int s_prefix[kMaxChunks + 1];
   __shared__ int s_hdr[6];
 
@@ -313,6 +322,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const float dx = a.dx;
   const float dx_inv = 1.f / dx;  // in-kernel, as the reference (:276-277)
   const float dt_inv = 1.f / dt;
+  const float fric_u = dt * kG / (a.kst_fixed * a.kst_fixed);  // uniform kSt: dt * G / (kSt * kSt)
   const int W = a.W, H = a.H, pitch = a.pitch;
   const float nv = a.no_value;
   const int scol = FIP_SMEM_X0 - 4 + 120 * warp + 4 * lane;  // staged column of k = 0
@@ -324,21 +334,26 @@ __global__ void __launch_bounds__(kThreads, 2)
   unsigned char* const nzs = a.nz[it & 1];
 
   float cfl = 1.0f;
-  bool bad = false;
+  unsigned expacc = 0u;  // largest exponent field of a computed depth
   uint32_t seq = 0;
   Walk w = walk0;
   int s, ra, rb;
   while (next_run(w, list, s_prefix, a.n_chunks, a.n_ty, H, &s, &ra, &rb)) {
     const int c = s * FIP_TILE_COLS - 4 + 120 * warp + 4 * lane;  // global column of k = 0
-    bool colH[4], colQX[4], colQY[4], holdX[4], colIn[4];
+    // 4-bit column masks of the cell sets the reference's kernel writes (src/kernels.cu:383-406)
+    int colHm = 0, colQXm = 0, colQYm = 0, colInm = 0;
+    bool holdX[4];
+    unsigned inmask[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int cc = c + k;
-      colH[k] = out_lane && cc >= 1 && cc <= W - 2;
-      colQX[k] = out_lane && cc >= 1 && cc <= W - 3;
-      colQY[k] = out_lane && cc >= 2 && cc <= W - 3;
+      colHm |= (out_lane && cc >= 1 && cc <= W - 2) << k;
+      colQXm |= (out_lane && cc >= 1 && cc <= W - 3) << k;
+      colQYm |= (out_lane && cc >= 2 && cc <= W - 3) << k;
+      const bool in = out_lane && cc >= 0 && cc < W;
+      colInm |= in << k;
+      inmask[k] = in ? 0x7fffffffu : 0u;
       holdX[k] = (cc == 0 || cc == W - 2);
-      colIn[k] = out_lane && cc >= 0 && cc < W;
     }
     const uint32_t seq0 = seq;
     auto slot_of = [&](int row) -> const unsigned char* {
@@ -360,38 +375,34 @@ __global__ void __launch_bounds__(kThreads, 2)
       break;
     }
     // ---- prologue: rows ra-2 .. ra ----
-    float h0[4], h1[4], hE0, hE1;
-    float qx0[4], qxW0, qy0[4], qyE0, qyS[4], qySE, s0[4], sE0;
+    // carried from row to row: only computed quantities; the raw fields of rows r-1 .. r+2 are
+    // read from the staged rows again at every row
     float ux0[4], uxW0, uy0[4], uyE0, uyS[4], gxS[4], gy0[4], qy2S[4];
+    float lim0[4], limE0;  // h * dt_inv * dx * 0.25f of row r (and its east neighbour)
     {
       const float4 vhs = lds4(slot_of(ra - 2), F_H, scol);
       const float4 vqys = lds4(slot_of(ra - 2), F_QY, scol);
       const float4 vh0 = lds4(slot_of(ra - 1), F_H, scol);
       const float4 vqx0 = lds4(slot_of(ra - 1), F_QX, scol);
       const float4 vqy0 = lds4(slot_of(ra - 1), F_QY, scol);
-      const float4 vs0 = lds4(slot_of(ra - 1), F_S, scol);
       const float4 vh1 = lds4(slot_of(ra), F_H, scol);
       const float hs[4] = {vhs.x, vhs.y, vhs.z, vhs.w};
-      qyS[0] = vqys.x; qyS[1] = vqys.y; qyS[2] = vqys.z; qyS[3] = vqys.w;
-      h0[0] = vh0.x; h0[1] = vh0.y; h0[2] = vh0.z; h0[3] = vh0.w;
-      qx0[0] = vqx0.x; qx0[1] = vqx0.y; qx0[2] = vqx0.z; qx0[3] = vqx0.w;
-      qy0[0] = vqy0.x; qy0[1] = vqy0.y; qy0[2] = vqy0.z; qy0[3] = vqy0.w;
-      s0[0] = vs0.x; s0[1] = vs0.y; s0[2] = vs0.z; s0[3] = vs0.w;
-      h1[0] = vh1.x; h1[1] = vh1.y; h1[2] = vh1.z; h1[3] = vh1.w;
-      qySE = __shfl_down_sync(0xffffffffu, qyS[0], 1);
-      hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
-      qxW0 = __shfl_up_sync(0xffffffffu, qx0[3], 1);
-      qyE0 = __shfl_down_sync(0xffffffffu, qy0[0], 1);
-      sE0 = __shfl_down_sync(0xffffffffu, s0[0], 1);
-      hE1 = __shfl_down_sync(0xffffffffu, h1[0], 1);
+      const float qyS[4] = {vqys.x, vqys.y, vqys.z, vqys.w};
+      const float h0[4] = {vh0.x, vh0.y, vh0.z, vh0.w};
+      const float qx0[4] = {vqx0.x, vqx0.y, vqx0.z, vqx0.w};
+      const float qy0[4] = {vqy0.x, vqy0.y, vqy0.z, vqy0.w};
+      const float h1[4] = {vh1.x, vh1.y, vh1.z, vh1.w};
+      const float hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         uyS[k] = fdivw(qyS[k], fmaxf(fmaxf(kDH, hs[k]), h0[k]));
         ux0[k] = fdivw(qx0[k], fmaxf(fmaxf(kDH, h0[k]), k < 3 ? h0[k + 1] : hE0));
         uy0[k] = fdivw(qy0[k], fmaxf(fmaxf(kDH, h0[k]), h1[k]));
+        lim0[k] = h0[k] * dt_inv * dx * 0.25f;
       }
       uxW0 = __shfl_up_sync(0xffffffffu, ux0[3], 1);
       uyE0 = __shfl_down_sync(0xffffffffu, uy0[0], 1);
+      limE0 = __shfl_down_sync(0xffffffffu, lim0[0], 1);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         // compute_rmg_gy for row ra-1: uy_i = uy(ra-1), uy_south = uy(ra-2)
@@ -400,20 +411,33 @@ __global__ void __launch_bounds__(kThreads, 2)
         qy2S[k] = 0.f;
       }
     }
-    release_row(ra - 2);
-
-    bool nzf = false;
+    // rows r-1 .. r+2 stay staged during row r: qy(r-1) and the terrain of row r are read
+    // again instead of being carried in registers; row r-1 is released at the end of row r
+    unsigned nzacc = 0u;
     for (int r = ra - 1; r < rb; ++r) {
       if (!wait_row(r + 2)) {
         record_error(ctl, FIP_DEVERR_WAIT_FULL);
         ok = false;
         break;
       }
+      const unsigned char* slS = slot_of(r - 1);
       const unsigned char* sl0 = slot_of(r);
       const unsigned char* sl1 = slot_of(r + 1);
       const unsigned char* sl2 = slot_of(r + 2);
-      float h2r[4], qx1[4], qy1[4], s1[4], kk[4];
+      float h2r[4], qx1[4], qy1[4], s1[4], fric[4], qyS[4], s0[4], h0[4], h1[4], qx0[4], qy0[4];
       {
+        const float4 vqs = lds4(slS, F_QY, scol);
+        const float4 vs0 = lds4(sl0, F_S, scol);
+        const float4 vh0 = lds4(sl0, F_H, scol);
+        const float4 vqx0 = lds4(sl0, F_QX, scol);
+        const float4 vqy0 = lds4(sl0, F_QY, scol);
+        const float4 vh1 = lds4(sl1, F_H, scol);
+        qyS[0] = vqs.x; qyS[1] = vqs.y; qyS[2] = vqs.z; qyS[3] = vqs.w;
+        s0[0] = vs0.x; s0[1] = vs0.y; s0[2] = vs0.z; s0[3] = vs0.w;
+        h0[0] = vh0.x; h0[1] = vh0.y; h0[2] = vh0.z; h0[3] = vh0.w;
+        qx0[0] = vqx0.x; qx0[1] = vqx0.y; qx0[2] = vqx0.z; qx0[3] = vqx0.w;
+        qy0[0] = vqy0.x; qy0[1] = vqy0.y; qy0[2] = vqy0.z; qy0[3] = vqy0.w;
+        h1[0] = vh1.x; h1[1] = vh1.y; h1[2] = vh1.z; h1[3] = vh1.w;
         const float4 v2 = lds4(sl2, F_H, scol);
         const float4 vqx = lds4(sl1, F_QX, scol);
         const float4 vqy = lds4(sl1, F_QY, scol);
@@ -424,23 +448,28 @@ __global__ void __launch_bounds__(kThreads, 2)
         s1[0] = vs.x; s1[1] = vs.y; s1[2] = vs.z; s1[3] = vs.w;
         if (KVAR) {
           const float4 vk = lds4(sl0, F_K, scol);
-          kk[0] = vk.x; kk[1] = vk.y; kk[2] = vk.z; kk[3] = vk.w;
+          const float kk[4] = {vk.x, vk.y, vk.z, vk.w};
+#pragma unroll
+          for (int k = 0; k < 4; ++k) fric[k] = dt * kG / (kk[k] * kk[k]);
         } else {
-          kk[0] = kk[1] = kk[2] = kk[3] = a.kst_fixed;
+          fric[0] = fric[1] = fric[2] = fric[3] = fric_u;
         }
       }
-      release_row(r);
-      const float hE2 = __shfl_down_sync(0xffffffffu, h2r[0], 1);
+      const float hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
+      const float hE1 = __shfl_down_sync(0xffffffffu, h1[0], 1);
+      const float qxW0 = __shfl_up_sync(0xffffffffu, qx0[3], 1);
+      const float qyE0 = __shfl_down_sync(0xffffffffu, qy0[0], 1);
+      const float qySE = __shfl_down_sync(0xffffffffu, qyS[0], 1);
+      const float sE0 = __shfl_down_sync(0xffffffffu, s0[0], 1);
       const float qxW1 = __shfl_up_sync(0xffffffffu, qx1[3], 1);
-      const float qyE1 = __shfl_down_sync(0xffffffffu, qy1[0], 1);
-      const float sE1 = __shfl_down_sync(0xffffffffu, s1[0], 1);
 
-      // velocities of row r+1 (src/kernels.cu:351-354)
-      float ux1[4], uy1[4];
+      // velocities of row r+1 (src/kernels.cu:351-354) and the clamp factors of row r+1
+      float ux1[4], uy1[4], lim1[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         ux1[k] = fdivw(qx1[k], fmaxf(fmaxf(kDH, h1[k]), k < 3 ? h1[k + 1] : hE1));
         uy1[k] = fdivw(qy1[k], fmaxf(fmaxf(kDH, h1[k]), h2r[k]));
+        lim1[k] = h1[k] * dt_inv * dx * 0.25f;
       }
       const float ux1W = __shfl_up_sync(0xffffffffu, ux1[3], 1);
       const float uy1E = __shfl_down_sync(0xffffffffu, uy1[0], 1);
@@ -466,72 +495,86 @@ __global__ void __launch_bounds__(kThreads, 2)
       const float fxE = __shfl_down_sync(0xffffffffu, fx[0], 1);
 
       const bool hold_y = (r == 0 || r == H - 2);
+      // face depths and the discharge magnitudes the friction factor uses (:83-92, :110-119)
+      float ax0[4], ax1[4], ay0[4], ay1[4], uyx[4], uxy[4];
+      bool movex[4], movey[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        ax0[k] = fmaxf(0.f, (h0[k] + (k < 3 ? h0[k + 1] : hE0)) * .5f);
+        ax1[k] = fmaxf(ax0[k], kDH);
+        ay0[k] = fmaxf(0.f, (h0[k] + h1[k]) * .5f);
+        ay1[k] = fmaxf(ay0[k], kDH);
+        uyx[k] = (qy0[k] + (k < 3 ? qy0[k + 1] : qyE0) + qyS[k] + (k < 3 ? qyS[k + 1] : qySE)) * 0.25f;
+        uxy[k] = (qx0[k] + qx1[k] + (k > 0 ? qx0[k - 1] : qxW0) + (k > 0 ? qx1[k - 1] : qxW1)) * 0.25f;
+        movex[k] = !((qx0[k] == 0.f) & (uyx[k] == 0.f));
+        movey[k] = !((uxy[k] == 0.f) & (qy0[k] == 0.f));
+      }
+      float rx[4], ry[4];  // friction factors, 0 where the discharges vanish (:93, :120)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float fxk = friction(fric[k], qx0[k], uyx[k], ax1[k]);
+        const float fyk = friction(fric[k], uxy[k], qy0[k], ay1[k]);
+        rx[k] = movex[k] ? fxk : 0.f;
+        ry[k] = movey[k] ? fyk : 0.f;
+      }
       float qx2[4], qy2[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const float fq = upd_qx(k < 3 ? fx[k + 1] : fxE, fx[k], gx[k], gxS[k], dt, dx, dt_inv, dx_inv, kk[k], h0[k],
-                                k < 3 ? h0[k + 1] : hE0, k < 3 ? s0[k + 1] : sE0, s0[k], qx0[k], qy0[k],
-                                k < 3 ? qy0[k + 1] : qyE0, qyS[k], k < 3 ? qyS[k + 1] : qySE);
-        const float gq = upd_qy(fy[k], k > 0 ? fy[k - 1] : fyW, gy0[k], gy1[k], dt, dx, dt_inv, dx_inv, kk[k], h0[k],
-                                h1[k], s1[k], s0[k], qy0[k], qx0[k], k > 0 ? qx0[k - 1] : qxW0, qx1[k],
-                                k > 0 ? qx1[k - 1] : qxW1);
+        const float fq = upd_qx(k < 3 ? fx[k + 1] : fxE, fx[k], gx[k], gxS[k], dt, dx_inv, rx[k], ax0[k], h0[k],
+                                k < 3 ? h0[k + 1] : hE0, k < 3 ? s0[k + 1] : sE0, s0[k], qx0[k], lim0[k],
+                                k < 3 ? lim0[k + 1] : limE0);
+        const float gq = upd_qy(fy[k], k > 0 ? fy[k - 1] : fyW, gy0[k], gy1[k], dt, dx_inv, ry[k], ay0[k], h0[k],
+                                h1[k], s1[k], s0[k], qy0[k], lim0[k], lim1[k]);
         qx2[k] = holdX[k] ? qx0[k] : fq;  // boundary-face holds (:373-376)
         qy2[k] = hold_y ? qy0[k] : gq;
       }
       const float qx2W = __shfl_up_sync(0xffffffffu, qx2[3], 1);
 
-      if (r >= ra) {
-        const bool rowH = (r >= 1 && r <= H - 2);
-        const bool rowQX = (r >= 2 && r <= H - 3);
-        const bool rowQY = (r >= 1 && r <= H - 3);
+      {
+        const bool store_row = r >= ra;  // the extra row below a run only feeds qy2S
+        int validm = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) validm |= (s0[k] != nv) << k;
+        const int mH = (store_row && r >= 1 && r <= H - 2) ? (colHm & validm) : 0;
+        const int mQX = (store_row && r >= 2 && r <= H - 3) ? (colQXm & validm) : 0;
+        const int mQY = (store_row && r >= 1 && r <= H - 3) ? (colQYm & validm) : 0;
         float h2[4];
-        bool wH[4], wQX[4], wQY[4];
-        bool allH = true, allQX = true, allQY = true;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           h2[k] = h0[k] - dt * dx_inv * ((qx2[k] - (k > 0 ? qx2[k - 1] : qx2W)) + (qy2[k] - qy2S[k]));
-          const bool valid = (s0[k] != nv);
-          wH[k] = rowH && colH[k] && valid;
-          wQX[k] = rowQX && colQX[k] && valid;
-          wQY[k] = rowQY && colQY[k] && valid;
-          allH &= wH[k];
-          allQX &= wQX[k];
-          allQY &= wQY[k];
-          if (wH[k]) {
-            bad |= !(fabsf(h2[k]) <= 3.402823466e38f);
-            if (h2[k] > kEPS) {  // CFL of wet stored cells (:392-396), velocities of the old state
-              const float uw = k > 0 ? ux0[k - 1] : uxW0;
-              const float umax = fmaxf(fabsf(uy0[k]), fmaxf(fabsf(uyS[k]), fmaxf(fabsf(ux0[k]), fabsf(uw))));
-              const float dtc = dx / (sqrtf(kG * h2[k]) + umax);
-              cfl = fminf(cfl, dtc);
-            }
-          }
-          if (colIn[k]) nzf |= (h2[k] != 0.f) | (qx2[k] != 0.f) | (qy2[k] != 0.f);
+          const bool wk = (mH >> k) & 1;
+          expacc = max(expacc, __float_as_uint(h2[k]) & 0x7f800000u);  // all-ones exponent: NaN/Inf
+          // CFL of wet stored cells (:392-396), velocities of the old state
+          const float uw = k > 0 ? ux0[k - 1] : uxW0;
+          const float umax = fmaxf(fabsf(uy0[k]), fmaxf(fabsf(uyS[k]), fmaxf(fabsf(ux0[k]), fabsf(uw))));
+          const float dtc = dx / (sqrtf(kG * h2[k]) + umax);
+          cfl = fminf(cfl, (wk && h2[k] > kEPS) ? dtc : 1.0f);
+          nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & inmask[k];
         }
         const size_t row_off = (size_t)r * (size_t)pitch + (size_t)c;
-        if (allH) {
+        if (mH == 15) {
           *reinterpret_cast<float4*>(h_out + row_off) = make_float4(h2[0], h2[1], h2[2], h2[3]);
         } else {
 #pragma unroll
           for (int k = 0; k < 4; ++k)
-            if (wH[k]) h_out[row_off + k] = h2[k];
+            if ((mH >> k) & 1) h_out[row_off + k] = h2[k];
         }
-        if (allQX) {
+        if (mQX == 15) {
           *reinterpret_cast<float4*>(qx_out + row_off) = make_float4(qx2[0], qx2[1], qx2[2], qx2[3]);
         } else {
 #pragma unroll
           for (int k = 0; k < 4; ++k)
-            if (wQX[k]) qx_out[row_off + k] = qx2[k];
+            if ((mQX >> k) & 1) qx_out[row_off + k] = qx2[k];
         }
-        if (allQY) {
+        if (mQY == 15) {
           *reinterpret_cast<float4*>(qy_out + row_off) = make_float4(qy2[0], qy2[1], qy2[2], qy2[3]);
         } else {
 #pragma unroll
           for (int k = 0; k < 4; ++k)
-            if (wQY[k]) qy_out[row_off + k] = qy2[k];
+            if ((mQY >> k) & 1) qy_out[row_off + k] = qy2[k];
         }
-        if (fold) {  // flood_plains_kernel on the post-boundary state of the last step (:254-262)
-          if (colIn[0] && colIn[3]) {
+        if (fold && store_row) {  // flood_plains_kernel on the post-boundary state of the last step (:254-262)
+          if (colInm == 15) {
             float4* hm = reinterpret_cast<float4*>(a.hmax + row_off);
             float4 m = *hm;
             m.x = fmaxf(m.x, h0[0]);
@@ -542,42 +585,35 @@ __global__ void __launch_bounds__(kThreads, 2)
           } else {
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-              if (colIn[k]) a.hmax[row_off + k] = fmaxf(a.hmax[row_off + k], h0[k]);
+              if ((colInm >> k) & 1) a.hmax[row_off + k] = fmaxf(a.hmax[row_off + k], h0[k]);
           }
         }
         // per-tile wet flag for the next plan, flushed at the tile's last row
-        if ((r + 1) % FIP_TILE_ROWS == 0 || r + 1 == rb) {
-          if (__any_sync(0xffffffffu, nzf) && lane == 0) nzs[s * a.n_ty + r / FIP_TILE_ROWS] = 1;
-          nzf = false;
+        if (store_row && ((r + 1) % FIP_TILE_ROWS == 0 || r + 1 == rb)) {
+          if (__any_sync(0xffffffffu, nzacc != 0u) && lane == 0) nzs[s * a.n_ty + r / FIP_TILE_ROWS] = 1;
+          nzacc = 0u;
         }
       }
 
+      nzacc = store_row_flag(r, ra) ? nzacc : 0u;  // the extra row below a run is no part of a tile
+      release_row(r - 1);
       // travel north (:408-433)
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         qy2S[k] = qy2[k];
-        qyS[k] = qy0[k];
         gxS[k] = gx[k];
         uyS[k] = uy0[k];
-        h0[k] = h1[k];
-        h1[k] = h2r[k];
-        qx0[k] = qx1[k];
-        qy0[k] = qy1[k];
-        s0[k] = s1[k];
         ux0[k] = ux1[k];
         uy0[k] = uy1[k];
         gy0[k] = gy1[k];
+        lim0[k] = lim1[k];
       }
-      qySE = qyE0;
-      hE0 = hE1;
-      hE1 = hE2;
-      qxW0 = qxW1;
-      qyE0 = qyE1;
-      sE0 = sE1;
       uxW0 = ux1W;
       uyE0 = uy1E;
+      limE0 = __shfl_down_sync(0xffffffffu, lim0[0], 1);
     }
     if (!ok) break;
+    release_row(rb - 1);
     release_row(rb);
     release_row(rb + 1);
     seq += (uint32_t)(rb - ra + 4);
@@ -607,7 +643,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   // CFL minimum: warp reduction, one atomicMin per warp on the float bits (all positive)
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) cfl = fminf(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
-  const bool any_bad = __any_sync(0xffffffffu, bad);
+  const bool any_bad = __any_sync(0xffffffffu, expacc == 0x7f800000u);
   if (lane == 0) {
     if (cfl < 1.0f) atomicMin(&ctl->cfl_bits[it & 1], __float_as_uint(cfl));
     if (any_bad) ctl->nonfinite = 1;
@@ -734,12 +770,13 @@ int make_tensor_maps(StencilState* st) {
 int rmg_step_grid(int device) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return 2 * sms;
+  return kMinCtas * sms;
 }
 
 template <bool KVAR>
 static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t stream) {
   constexpr int NF = KVAR ? 5 : 4;
+  constexpr int kNSlot = KVAR ? FIP_NSLOT_KVAR : FIP_NSLOT_UNIFORM;
   const int smem = kNSlot * NF * kFieldBytes + 1024;
   static bool configured = false;
   if (!configured) {

@@ -53,7 +53,7 @@ cudaError_t launch_volume(const StencilState& st, int parity, double* partials, 
 cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, const int* xy_type,
                                  float* out, cudaStream_t stream);
 
-// Number of CTAs the step kernel runs with (2 per SM).
+// Number of CTAs the step kernel runs with (3 per SM).
 int rmg_step_grid(int device);
 
 }  // namespace fip
