@@ -36,6 +36,22 @@ __device__ __forceinline__ float fip_interp(const float* tv, int n, float time) 
   return __fadd_rn(__fmul_rn(f, tv[n + lo]), __fmul_rn(__fsub_rn(1.f, f), tv[n + lo - 1]));
 }
 
+// TimeSeries::interp with the whole block finding the bracket: lower_bound = number of table
+// times below `time` (one __syncthreads_count per 512 entries instead of a chain of dependent
+// loads); every thread returns the same value.
+__device__ float fip_interp_block(const float* tv, int n, float time) {
+  int lo = 0;
+  for (int j0 = 0; j0 < n; j0 += blockDim.x) {
+    const int j = j0 + threadIdx.x;
+    lo += __syncthreads_count(j < n && tv[j] < time);
+  }
+  if (lo == 0) return tv[n];
+  if (lo == n) return tv[2 * n - 1];
+  const float dt = __fsub_rn(tv[lo], tv[lo - 1]);
+  const float f = __fdiv_rn(__fsub_rn(time, tv[lo - 1]), dt);
+  return __fadd_rn(__fmul_rn(f, tv[n + lo]), __fmul_rn(__fsub_rn(1.f, f), tv[n + lo - 1]));
+}
+
 // sequential float sum of sqrt(g a) a over the condition's cells [from, to), a = z - terrain
 // (0 below 1 cm), times dx. Terms are evaluated in parallel, summed in order by thread 0.
 __device__ float fip_sum_depths(const float* sohle, long long base, long long inc, int from, int to, float z,
@@ -201,82 +217,98 @@ const char* type_name(BcType t) {
   }
 }
 
-// src_side_* (src/bc_kernel_gen.cpp:11-73): cell, staggered face and inner neighbour
-void emit_side(std::ostream& o, BcSide side) {
+// src_side_* (src/bc_kernel_gen.cpp:11-73): the side's cell, staggered face and inner
+// neighbour of boundary cell `tid`, and the discharge arrays (normal q, lateral q_lateral)
+struct SideExpr {
+  const char *idx, *stag, *nb, *q, *q_lateral;
+};
+SideExpr side_expr(BcSide side) {
   switch (side) {
-    case BcSide::right:
-      o << "      const long long idx = tid * pitch + W - 1;\n"
-           "      const long long idx_staggered = idx - 1;\n"
-           "      const long long idx_neighbor = idx - 1;\n"
-           "      float* q = qx;\n      float* q_lateral = qy;\n";
-      break;
-    case BcSide::left:
-      o << "      const long long idx = tid * pitch;\n"
-           "      const long long idx_staggered = idx;\n"
-           "      const long long idx_neighbor = idx + 1;\n"
-           "      float* q = qx;\n      float* q_lateral = qy;\n";
-      break;
-    case BcSide::top:
-      o << "      const long long idx = tid + (H - 1) * pitch;\n"
-           "      const long long idx_staggered = idx - pitch;\n"
-           "      const long long idx_neighbor = idx - pitch;\n"
-           "      float* q = qy;\n      float* q_lateral = qx;\n";
-      break;
-    case BcSide::bottom:
-      o << "      const long long idx = tid;\n"
-           "      const long long idx_staggered = idx;\n"
-           "      const long long idx_neighbor = idx + pitch;\n"
-           "      float* q = qy;\n      float* q_lateral = qx;\n";
-      break;
+    case BcSide::right: return {"tid * pitch + W - 1", "idx - 1", "idx - 1", "qx", "qy"};
+    case BcSide::left: return {"tid * pitch", "idx", "idx + 1", "qx", "qy"};
+    case BcSide::top: return {"tid + (H - 1) * pitch", "idx - pitch", "idx - pitch", "qy", "qx"};
+    default: return {"tid", "idx", "idx + pitch", "qy", "qx"};
   }
-  o << "      (void)idx_staggered; (void)q_lateral;\n";
 }
 
-// src_type_* (src/bc_kernel_gen.cpp:75-137); `staggered` for the rmg solver
-void emit_type(std::ostream& o, BcType type, bool staggered) {
-  const char* qi = staggered ? "idx_staggered" : "idx";
-  switch (type) {
+// One condition's cell loop. Cells of one condition never touch each other's cells, so each
+// thread first loads the operands of 4 cells and then stores them, which lets the loads of the
+// 4 cells overlap. The arithmetic is the reference's fragment (src_type_*, src/bc_kernel_gen.cpp:
+// 75-137) verbatim in effect: no multiply-add pairs, IEEE sqrtf, so the same rounding.
+void emit_cells(std::ostream& o, const BoundaryCondition& bc, bool staggered) {
+  const SideExpr e = side_expr(bc.side);
+  const char* qi = staggered ? "stg[u]" : "ci[u]";
+  o << "      float* const q = " << e.q << ";\n      float* const q_lateral = " << e.q_lateral << ";\n";
+  o << "      (void)q_lateral;\n";
+  o << "      for (long long t0 = " << bc.from << "; t0 <= " << bc.to << "; t0 += 4LL * FIP_POST_THREADS) {\n";
+  o << "        long long ci[4], stg[4], nbr[4];\n        bool on[4];\n        float L0[4], L1[4], L2[4];\n        (void)L2;\n";
+  o << "#pragma unroll\n        for (int u = 0; u < 4; ++u) {\n";
+  o << "          const long long tid = t0 + (long long)u * FIP_POST_THREADS + threadIdx.x;\n";
+  o << "          on[u] = tid <= " << bc.to << ";\n";
+  o << "          const long long idx = " << e.idx << ";\n";
+  o << "          ci[u] = idx;\n          stg[u] = " << e.stag << ";\n          nbr[u] = " << e.nb << ";\n";
+  o << "          L0[u] = L1[u] = L2[u] = 0.f;\n";
+  o << "          if (on[u]) {\n";
+  switch (bc.type) {
     case BcType::z:
-      if (staggered)
-        o << "      h[idx] = fmaxf(0.f, zval - sohle[idx]);\n"
-             "      h[idx_neighbor] = fmaxf(0.f, zval - sohle[idx_neighbor]);\n"
-             "      q[idx_staggered] = -0.f;\n";
-      else
-        o << "      const float ah = fmaxf(0.f, zval - sohle[idx]);\n"
-             "      h[idx] = ah;\n"
-             "      q[idx] = 0.99f * (q[idx_neighbor] / fmaxf(h[idx_neighbor], 0.01f)) * ah;\n";
+      if (staggered) o << "            L0[u] = sohle[ci[u]]; L1[u] = sohle[nbr[u]];\n";
+      else o << "            L0[u] = sohle[ci[u]]; L1[u] = q[nbr[u]]; L2[u] = h[nbr[u]];\n";
       break;
     case BcType::q:
-      o << "      float ah = zval - sohle[idx];\n"
-           "      if (ah < 0.f) ah = 0.f;\n"
-           "      q["
-        << qi << "] = sqrtf(FIP_G * ah) * ah * qval;\n";
-      if (staggered)
-        o << "      if (ah > 0.f) {\n"
-             "        const float z_neighbor = h[idx_neighbor] + sohle[idx_neighbor];\n"
-             "        h[idx] = fmaxf(ah / 2, z_neighbor - sohle[idx]);\n"
-             "      }\n";
-      else
-        o << "      if (ah > 0.f) h[idx] = fmaxf(ah / 2, h[idx_neighbor] + sohle[idx_neighbor] - sohle[idx]);\n";
+      o << "            L0[u] = sohle[ci[u]]; L1[u] = h[nbr[u]]; L2[u] = sohle[nbr[u]];\n";
       break;
     case BcType::close:
-      o << "      q[" << qi
-        << "] = 0.f;\n"
-           "      q_lateral[idx] = q_lateral[idx_neighbor];\n"
-           "      h[idx] = h[idx_neighbor];\n";
+      o << "            L0[u] = q_lateral[nbr[u]]; L1[u] = h[nbr[u]];\n";
       break;
     case BcType::open:
-      o << "      const float ah_neighbor = h[idx_neighbor];\n"
-           "      const float z_neighbor = ah_neighbor + sohle[idx_neighbor];\n"
-           "      const float sign = (float)(idx - idx_neighbor);\n"
-           "      if (ah_neighbor > 0.f) {\n"
-           "        q["
-        << qi
-        << "] = sign * sqrtf(FIP_G * ah_neighbor) * ah_neighbor;\n"
-           "        h[idx] = fminf(ah_neighbor, fmaxf(0.f, z_neighbor - sohle[idx]));\n"
-           "      }\n";
+      o << "            L0[u] = h[nbr[u]]; L1[u] = sohle[nbr[u]]; L2[u] = sohle[ci[u]];\n";
       break;
   }
+  o << "          }\n        }\n";
+  o << "#pragma unroll\n        for (int u = 0; u < 4; ++u) {\n          if (!on[u]) continue;\n";
+  switch (bc.type) {
+    case BcType::z:
+      if (staggered)
+        o << "          h[ci[u]] = fmaxf(0.f, zval - L0[u]);\n"
+             "          h[nbr[u]] = fmaxf(0.f, zval - L1[u]);\n"
+             "          q[stg[u]] = -0.f;\n";
+      else
+        o << "          const float ah = fmaxf(0.f, zval - L0[u]);\n"
+             "          h[ci[u]] = ah;\n"
+             "          q[ci[u]] = 0.99f * (L1[u] / fmaxf(L2[u], 0.01f)) * ah;\n";
+      break;
+    case BcType::q:
+      o << "          float ah = zval - L0[u];\n"
+           "          if (ah < 0.f) ah = 0.f;\n"
+           "          q["
+        << qi << "] = sqrtf(FIP_G * ah) * ah * qval;\n";
+      if (staggered)
+        o << "          if (ah > 0.f) {\n"
+             "            const float z_neighbor = L1[u] + L2[u];\n"
+             "            h[ci[u]] = fmaxf(ah / 2, z_neighbor - L0[u]);\n"
+             "          }\n";
+      else
+        o << "          if (ah > 0.f) h[ci[u]] = fmaxf(ah / 2, L1[u] + L2[u] - L0[u]);\n";
+      break;
+    case BcType::close:
+      o << "          q[" << qi
+        << "] = 0.f;\n"
+           "          q_lateral[ci[u]] = L0[u];\n"
+           "          h[ci[u]] = L1[u];\n";
+      break;
+    case BcType::open:
+      o << "          const float ah_neighbor = L0[u];\n"
+           "          const float z_neighbor = ah_neighbor + L1[u];\n"
+           "          const float sign = (float)(ci[u] - nbr[u]);\n"
+           "          if (ah_neighbor > 0.f) {\n"
+           "            q["
+        << qi
+        << "] = sign * sqrtf(FIP_G * ah_neighbor) * ah_neighbor;\n"
+           "            h[ci[u]] = fminf(ah_neighbor, fmaxf(0.f, z_neighbor - L2[u]));\n"
+           "          }\n";
+      break;
+  }
+  o << "        }\n      }\n";
 }
 
 }  // namespace
@@ -315,12 +347,10 @@ std::string post_kernel_source(const Config& cfg, const SeriesLayout& ser, int p
       o << "      const float qval = " << flit(cfg.const_q(bc)) << ";\n";
     } else {
       // getZ / getQ of BoundaryConditionTimeseries (src/boundary_condition.cpp:56-77)
-      o << "      if (threadIdx.x == 0) s_val[0] = ";
       if (ser.z_off[i] >= 0)
-        o << "fip_interp(a.series + " << ser.z_off[i] << "L, " << ser.z_n[i] << ", t);\n";
+        o << "      const float zval = fip_interp_block(a.series + " << ser.z_off[i] << "L, " << ser.z_n[i] << ", t);\n";
       else
-        o << "0.f;\n";
-      o << "      __syncthreads();\n      const float zval = s_val[0];\n";
+        o << "      const float zval = 0.f;\n";
       if (bc.type == BcType::q) {
         long long base = 0, inc = 1;
         switch (bc.side) {
@@ -331,19 +361,16 @@ std::string post_kernel_source(const Config& cfg, const SeriesLayout& ser, int p
         }
         o << "      const float wsum = fip_sum_depths(sohle, " << base << "LL, " << inc << "LL, " << bc.from << ", "
           << bc.to << ", zval, a.dx, s_buf);\n";
-        o << "      if (threadIdx.x == 0) s_val[1] = __fdiv_rn(fip_interp(a.series + " << ser.q_off[i] << "L, "
-          << ser.q_n[i] << ", t), wsum);\n";
-        o << "      __syncthreads();\n      const float qval = s_val[1];\n";
+        o << "      if (threadIdx.x == 0) s_val[1] = wsum;\n      __syncthreads();\n";
+        o << "      const float qval = __fdiv_rn(fip_interp_block(a.series + " << ser.q_off[i] << "L, " << ser.q_n[i]
+          << ", t), s_val[1]);\n";
       } else {
-        o << "      const float qval = 0.f;\n";
+      o << "      const float qval = 0.f;\n";
       }
     }
     o << "      (void)zval; (void)qval;\n";
-    o << "      for (long long tid = " << bc.from << " + (long long)threadIdx.x; tid <= " << bc.to
-      << "; tid += blockDim.x) {\n";
-    emit_side(o, bc.side);
-    emit_type(o, bc.type, cfg.staggered());
-    o << "      }\n      __syncthreads();\n    }\n";
+    emit_cells(o, bc, cfg.staggered());
+    o << "      __syncthreads();\n    }\n";
   }
   o << kPostKernelTail;
   return o.str();
