@@ -9,10 +9,10 @@
 //     sqrtf/powf/division are the same approximations);
 //   * the domain is cut into tiles of 480 columns x 32 rows. A CTA has four consumer warps
 //     (each thread owns 4 adjacent columns, a warp 128 columns of which the 120 inner ones are
-//     stored) and one producer warp that streams rows of h/qx/qy/terrain/kSt into an 8-slot
-//     shared-memory ring with TMA (cp.async.bulk.tensor, no multicast). Consumers march north
-//     row by row, keeping the vertical window in registers and exchanging east/west
-//     neighbours with warp shuffles;
+//     stored) and one producer warp that streams rows of h/qx/qy/terrain/kSt into a ring of 7
+//     rows (8 without kSt) in shared memory with TMA (cp.async.bulk.tensor, no multicast).
+//     Consumers march north row by row over the staged rows r-1 .. r+2, exchange east/west
+//     neighbours with warp shuffles and do the arithmetic on FP32x2 pairs of columns;
 //   * work = the concatenation of the active tiles' rows (strip-major), split evenly over the
 //     persistent CTAs, so vertically adjacent active tiles are marched without re-staging;
 //   * each CTA folds its CFL minimum into ctl->cfl_bits with one atomicMin per warp, marks the
@@ -37,17 +37,10 @@ namespace {
 constexpr float kDH = 0.01f;         // src/kernels.cu:23
 constexpr float kEPS = 10e-7f;       // src/kernels.cu:24 (EPS_TROCKEN)
 constexpr float kG = 9.81f;          // src/simdata.h:358
-#ifndef FIP_NSLOT_KVAR
-#define FIP_NSLOT_KVAR 7
-#endif
-#ifndef FIP_NSLOT_UNIFORM
-#define FIP_NSLOT_UNIFORM 8
-#endif
+constexpr int kNSlotKvar = 7;
+constexpr int kNSlotUniform = 8;
 constexpr int kNSlotMax = 8;  // ring depth in rows: 7 with the kSt field (3 CTAs per SM fit), else 8
-#ifndef FIP_MIN_CTAS
-#define FIP_MIN_CTAS 3
-#endif
-constexpr int kMinCtas = FIP_MIN_CTAS;  // resident CTAs per SM
+constexpr int kMinCtas = 3;  // resident CTAs per SM (128 registers per thread)
 constexpr int kFieldBytes = FIP_SMEM_COLS * 4;  // 2048 B per staged row of one field
 constexpr int kConsumerWarps = 4;
 constexpr int kThreads = (kConsumerWarps + 1) * 32;
@@ -117,47 +110,71 @@ __device__ __forceinline__ void tma_row(void* dst, const CUtensorMap* tm, int x,
 }
 __device__ __forceinline__ void record_error(FipCtl* ctl, int code) { atomicCAS(&ctl->error, 0, code); }
 
-// fp32div_wrapper (src/kernels.cu:30-33)
-__device__ __forceinline__ float fdivw(float a, float b) { return (a == 0.0f) ? 0.0f : (a / b); }
-
-// compute_rmg_qx / compute_rmg_qy (src/kernels.cu:75-127), split in two so that a warp can
-// skip the friction factor when none of its cells moves (the reference selects 0 there):
-//   mom_depth: a0 = max(0, mean depth of the face), a1 = max(a0, DH)
-//   friction : dt * G / (kSt * kSt) * sqrt(ux^2 + uy^2) * (1 / a1)^2.33, the caller selects 0
-//              when ux == 0 && uy == 0 (discharges, not velocities, :91-94)
-//   upd_q*   : the rest, same operand order as the reference so the same rounding.
-// lim_i = h_i * dt_inv * dx * 0.25f comes precomputed per cell; the east (north) clamp
-// -h_east * dt_inv * dx * 0.25f equals -lim of the east (north) cell exactly, since a negation
-// commutes with rounding.
-__device__ __forceinline__ float friction(float fric, float ux, float uy, float a1) {
-  const float inv = 1.f / a1;
-  return fric * sqrtf(ux * ux + uy * uy) * powf(inv, 2.33f);
+// FP32x2 arithmetic (sm_100 packed add/mul/fma): a thread owns 4 adjacent columns and applies
+// the same operation to all of them, so columns (0,1) and (2,3) go through one instruction each.
+// Each component is rounded to nearest with denormals flushed, exactly like the scalar
+// operations under -use_fast_math, so every column gets the scalar result. a - b is issued as
+// fma(b, -1, a), which rounds once like a subtraction.
+__device__ __forceinline__ uint64_t pk2(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
 }
-
-__device__ __forceinline__ float upd_qx(float fx_east, float fx_i, float gx_i, float gx_south, float dt, float dx_inv,
-                                        float reib, float a0, float h_i, float h_east, float s_east, float s_i,
-                                        float qx_i, float lim_i, float lim_e) {
-  float dfx = (fx_east - fx_i) * dx_inv;
-  float dgx = (gx_i - gx_south) * dx_inv;
-  float dhg = a0 * kG * (-s_east + s_i) * dx_inv;
-  float dhx = (0.5f * kG * h_east * h_east - 0.5f * kG * h_i * h_i) * dx_inv;
-  float q = fdivw(qx_i + dt * (-dfx - dgx - dhx + dhg), (1.f + reib));
-  q = fminf(q, lim_i);
-  q = fmaxf(q, -lim_e);
-  return q;
+__device__ __forceinline__ void un2(uint64_t v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
 }
-
-__device__ __forceinline__ float upd_qy(float fy_i, float fy_west, float gy_i, float gy_north, float dt, float dx_inv,
-                                        float reib, float a0, float h_i, float h_north, float s_north, float s_i,
-                                        float qy_i, float lim_i, float lim_n) {
-  float dgy = (gy_north - gy_i) * dx_inv;
-  float dfy = (fy_i - fy_west) * dx_inv;
-  float dhg = a0 * kG * (s_i - s_north) * dx_inv;
-  float dhy = (0.5f * kG * h_north * h_north - 0.5f * kG * h_i * h_i) * dx_inv;
-  float q = fdivw(qy_i + dt * (-dgy - dfy - dhy + dhg), (1 + reib));
-  q = fminf(q, lim_i);
-  q = fmaxf(q, -lim_n);
-  return q;
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+// d = a op b over the 4 columns; a float2 operand is the same pair for both halves
+#define FIP_V2(name, op)                                                                   \
+  __device__ __forceinline__ void name(float (&d)[4], const float (&a)[4], const float (&b)[4]) { \
+    un2(op(pk2(a[0], a[1]), pk2(b[0], b[1])), d[0], d[1]);                                \
+    un2(op(pk2(a[2], a[3]), pk2(b[2], b[3])), d[2], d[3]);                                \
+  }                                                                                        \
+  __device__ __forceinline__ void name(float (&d)[4], const float (&a)[4], float2 b) {    \
+    const uint64_t bb = pk2(b.x, b.y);                                                     \
+    un2(op(pk2(a[0], a[1]), bb), d[0], d[1]);                                              \
+    un2(op(pk2(a[2], a[3]), bb), d[2], d[3]);                                              \
+  }                                                                                        \
+  __device__ __forceinline__ void name(float (&d)[4], float2 a, const float (&b)[4]) {    \
+    const uint64_t aa = pk2(a.x, a.y);                                                     \
+    un2(op(aa, pk2(b[0], b[1])), d[0], d[1]);                                              \
+    un2(op(aa, pk2(b[2], b[3])), d[2], d[3]);                                              \
+  }
+FIP_V2(vadd, add2)
+FIP_V2(vsub, sub2)
+FIP_V2(vmul, mul2)
+#undef FIP_V2
+// d = a * b + c
+__device__ __forceinline__ void vfma(float (&d)[4], const float (&a)[4], const float (&b)[4], const float (&c)[4]) {
+  un2(fma2(pk2(a[0], a[1]), pk2(b[0], b[1]), pk2(c[0], c[1])), d[0], d[1]);
+  un2(fma2(pk2(a[2], a[3]), pk2(b[2], b[3]), pk2(c[2], c[3])), d[2], d[3]);
+}
+__device__ __forceinline__ void vfma(float (&d)[4], const float (&a)[4], float2 b, const float (&c)[4]) {
+  const uint64_t bb = pk2(b.x, b.y);
+  un2(fma2(pk2(a[0], a[1]), bb, pk2(c[0], c[1])), d[0], d[1]);
+  un2(fma2(pk2(a[2], a[3]), bb, pk2(c[2], c[3])), d[2], d[3]);
+}
+__device__ __forceinline__ void vfma(float (&d)[4], float2 a, const float (&b)[4], const float (&c)[4]) {
+  const uint64_t aa = pk2(a.x, a.y);
+  un2(fma2(aa, pk2(b[0], b[1]), pk2(c[0], c[1])), d[0], d[1]);
+  un2(fma2(aa, pk2(b[2], b[3]), pk2(c[2], c[3])), d[2], d[3]);
 }
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
@@ -216,7 +233,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
                     const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_k,
                     const StepArgs a) {
   constexpr int NF = KVAR ? 5 : 4;
-  constexpr int kNSlot = KVAR ? FIP_NSLOT_KVAR : FIP_NSLOT_UNIFORM;
+  constexpr int kNSlot = KVAR ? kNSlotKvar : kNSlotUniform;
   constexpr int kSlotBytes = NF * kFieldBytes;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t full_bar[kNSlotMax];
@@ -323,6 +340,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
   const float dx_inv = 1.f / dx;  // in-kernel, as the reference (:276-277)
   const float dt_inv = 1.f / dt;
   const float fric_u = dt * kG / (a.kst_fixed * a.kst_fixed);  // uniform kSt: dt * G / (kSt * kSt)
+  const float dtg = dt * kG;                                    // kSt_var: (dt * G) / (kSt * kSt)
   const int W = a.W, H = a.H, pitch = a.pitch;
   const float nv = a.no_value;
   const int scol = FIP_SMEM_X0 - 4 + 120 * warp + 4 * lane;  // staged column of k = 0
@@ -332,6 +350,16 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
   float* const qy_out = a.qy[par ^ 1];
   const float* const h_in = a.h[par];
   unsigned char* const nzs = a.nz[it & 1];
+  // broadcast operands of the packed arithmetic
+  const float2 c_dti = make_float2(dt_inv, dt_inv), c_dx = make_float2(dx, dx);
+  const float2 c_dxi = make_float2(dx_inv, dx_inv), c_ndxi = make_float2(-dx_inv, -dx_inv);
+  const float2 c_dt = make_float2(dt, dt);
+  const float dtdx = dt * dx_inv;  // dt * dx_inv of the continuity update (:381), left to right
+  const float2 c_ndtdx = make_float2(-dtdx, -dtdx);
+  const float2 c_q = make_float2(0.25f, 0.25f), c_h = make_float2(0.5f, 0.5f), c_one = make_float2(1.f, 1.f);
+  const float2 c_g = make_float2(kG, kG), c_zero = make_float2(0.f, 0.f);
+  constexpr float kHG = 0.5f * kG;  // the reference's 0.5f * kG prefix, folded at compile time
+  const float2 c_hg = make_float2(kHG, kHG), c_nhg = make_float2(-kHG, -kHG);
 
   float cfl = 1.0f;
   unsigned expacc = 0u;  // largest exponent field of a computed depth
@@ -343,7 +371,6 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
     // 4-bit column masks of the cell sets the reference's kernel writes (src/kernels.cu:383-406)
     int colHm = 0, colQXm = 0, colQYm = 0, colInm = 0;
     bool holdX[4];
-    unsigned inmask[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int cc = c + k;
@@ -352,24 +379,23 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
       colQYm |= (out_lane && cc >= 2 && cc <= W - 3) << k;
       const bool in = out_lane && cc >= 0 && cc < W;
       colInm |= in << k;
-      inmask[k] = in ? 0x7fffffffu : 0u;
       holdX[k] = (cc == 0 || cc == W - 2);
     }
-    const uint32_t seq0 = seq;
-    auto slot_of = [&](int row) -> const unsigned char* {
-      return ring + ((seq0 + (uint32_t)(row - (ra - 2))) % kNSlot) * kSlotBytes;
-    };
-    auto wait_row = [&](int row) -> bool {  // warp-uniform: every lane waits, all must succeed
-      const uint32_t q = seq0 + (uint32_t)(row - (ra - 2));
+    // ring slots of the staged rows r-1, r, r+1, r+2 (row ra-2 has sequence number seq); the
+    // row loop advances them by one slot per row
+    uint32_t iS = seq % kNSlot;
+    uint32_t i0 = (seq + 1) % kNSlot, i1 = (seq + 2) % kNSlot, i2 = (seq + 3) % kNSlot;
+    uint32_t ph2 = ((seq + 3) / kNSlot) & 1u;  // phase of the slot of row r+2
+    auto wait_slot = [&](uint32_t q) -> bool {  // warp-uniform: every lane waits, all must succeed
       const bool got = mbar_wait(&full_bar[q % kNSlot], (q / kNSlot) & 1u);
       return __all_sync(0xffffffffu, got);
     };
-    auto release_row = [&](int row) {
+    auto release_slot = [&](uint32_t slot) {
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty_bar[(seq0 + (uint32_t)(row - (ra - 2))) % kNSlot]);
+      if (lane == 0) mbar_arrive(&empty_bar[slot]);
     };
 
-    bool ok = wait_row(ra - 2) && wait_row(ra - 1) && wait_row(ra);
+    bool ok = wait_slot(seq) && wait_slot(seq + 1) && wait_slot(seq + 2);
     if (!ok) {
       record_error(ctl, FIP_DEVERR_WAIT_FULL);
       break;
@@ -380,12 +406,15 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
     float ux0[4], uxW0, uy0[4], uyE0, uyS[4], gxS[4], gy0[4], qy2S[4];
     float lim0[4], limE0;  // h * dt_inv * dx * 0.25f of row r (and its east neighbour)
     {
-      const float4 vhs = lds4(slot_of(ra - 2), F_H, scol);
-      const float4 vqys = lds4(slot_of(ra - 2), F_QY, scol);
-      const float4 vh0 = lds4(slot_of(ra - 1), F_H, scol);
-      const float4 vqx0 = lds4(slot_of(ra - 1), F_QX, scol);
-      const float4 vqy0 = lds4(slot_of(ra - 1), F_QY, scol);
-      const float4 vh1 = lds4(slot_of(ra), F_H, scol);
+      const unsigned char* slA = ring + iS * kSlotBytes;
+      const unsigned char* slB = ring + i0 * kSlotBytes;
+      const unsigned char* slC = ring + i1 * kSlotBytes;
+      const float4 vhs = lds4(slA, F_H, scol);
+      const float4 vqys = lds4(slA, F_QY, scol);
+      const float4 vh0 = lds4(slB, F_H, scol);
+      const float4 vqx0 = lds4(slB, F_QX, scol);
+      const float4 vqy0 = lds4(slB, F_QY, scol);
+      const float4 vh1 = lds4(slC, F_H, scol);
       const float hs[4] = {vhs.x, vhs.y, vhs.z, vhs.w};
       const float qyS[4] = {vqys.x, vqys.y, vqys.z, vqys.w};
       const float h0[4] = {vh0.x, vh0.y, vh0.z, vh0.w};
@@ -395,11 +424,13 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
       const float hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        uyS[k] = fdivw(qyS[k], fmaxf(fmaxf(kDH, hs[k]), h0[k]));
-        ux0[k] = fdivw(qx0[k], fmaxf(fmaxf(kDH, h0[k]), k < 3 ? h0[k + 1] : hE0));
-        uy0[k] = fdivw(qy0[k], fmaxf(fmaxf(kDH, h0[k]), h1[k]));
-        lim0[k] = h0[k] * dt_inv * dx * 0.25f;
+        uyS[k] = qyS[k] / fmaxf(fmaxf(kDH, hs[k]), h0[k]);
+        ux0[k] = qx0[k] / fmaxf(fmaxf(kDH, h0[k]), k < 3 ? h0[k + 1] : hE0);
+        uy0[k] = qy0[k] / fmaxf(fmaxf(kDH, h0[k]), h1[k]);
       }
+      vmul(lim0, h0, c_dti);
+      vmul(lim0, lim0, c_dx);
+      vmul(lim0, lim0, c_q);
       uxW0 = __shfl_up_sync(0xffffffffu, ux0[3], 1);
       uyE0 = __shfl_down_sync(0xffffffffu, uy0[0], 1);
       limE0 = __shfl_down_sync(0xffffffffu, lim0[0], 1);
@@ -415,15 +446,18 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
     // again instead of being carried in registers; row r-1 is released at the end of row r
     unsigned nzacc = 0u;
     for (int r = ra - 1; r < rb; ++r) {
-      if (!wait_row(r + 2)) {
-        record_error(ctl, FIP_DEVERR_WAIT_FULL);
-        ok = false;
-        break;
+      {  // wait for row r+2
+        const bool got = __all_sync(0xffffffffu, mbar_wait(&full_bar[i2], ph2));
+        if (!got) {
+          record_error(ctl, FIP_DEVERR_WAIT_FULL);
+          ok = false;
+          break;
+        }
       }
-      const unsigned char* slS = slot_of(r - 1);
-      const unsigned char* sl0 = slot_of(r);
-      const unsigned char* sl1 = slot_of(r + 1);
-      const unsigned char* sl2 = slot_of(r + 2);
+      const unsigned char* slS = ring + iS * kSlotBytes;
+      const unsigned char* sl0 = ring + i0 * kSlotBytes;
+      const unsigned char* sl1 = ring + i1 * kSlotBytes;
+      const unsigned char* sl2 = ring + i2 * kSlotBytes;
       float h2r[4], qx1[4], qy1[4], s1[4], fric[4], qyS[4], s0[4], h0[4], h1[4], qx0[4], qy0[4];
       {
         const float4 vqs = lds4(slS, F_QY, scol);
@@ -448,9 +482,10 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
         s1[0] = vs.x; s1[1] = vs.y; s1[2] = vs.z; s1[3] = vs.w;
         if (KVAR) {
           const float4 vk = lds4(sl0, F_K, scol);
-          const float kk[4] = {vk.x, vk.y, vk.z, vk.w};
+          float kk[4] = {vk.x, vk.y, vk.z, vk.w};
+          vmul(kk, kk, kk);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) fric[k] = dt * kG / (kk[k] * kk[k]);
+          for (int k = 0; k < 4; ++k) fric[k] = dtg / kk[k];
         } else {
           fric[0] = fric[1] = fric[2] = fric[3] = fric_u;
         }
@@ -462,71 +497,165 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
       const float qySE = __shfl_down_sync(0xffffffffu, qyS[0], 1);
       const float sE0 = __shfl_down_sync(0xffffffffu, s0[0], 1);
       const float qxW1 = __shfl_up_sync(0xffffffffu, qx1[3], 1);
+      float t[4], u[4];
 
       // velocities of row r+1 (src/kernels.cu:351-354) and the clamp factors of row r+1
       float ux1[4], uy1[4], lim1[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        ux1[k] = fdivw(qx1[k], fmaxf(fmaxf(kDH, h1[k]), k < 3 ? h1[k + 1] : hE1));
-        uy1[k] = fdivw(qy1[k], fmaxf(fmaxf(kDH, h1[k]), h2r[k]));
-        lim1[k] = h1[k] * dt_inv * dx * 0.25f;
+        ux1[k] = qx1[k] / fmaxf(fmaxf(kDH, h1[k]), k < 3 ? h1[k + 1] : hE1);
+        uy1[k] = qy1[k] / fmaxf(fmaxf(kDH, h1[k]), h2r[k]);
       }
+      vmul(lim1, h1, c_dti);
+      vmul(lim1, lim1, c_dx);
+      vmul(lim1, lim1, c_q);
       const float ux1W = __shfl_up_sync(0xffffffffu, ux1[3], 1);
       const float uy1E = __shfl_down_sync(0xffffffffu, uy1[0], 1);
 
       float fx[4], fy[4], gx[4], gy1[4];
+      // compute_rmg_fy (:45-54): ux at the cell and its north neighbour
+      vadd(t, ux0, ux1);
+      vmul(u, t, c_h);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) fy[k] = t[k] > 0 ? qy0[k] : (k < 3 ? qy0[k + 1] : qyE0);
+      vmul(fy, fy, u);
+      // compute_rmg_gy for row r+1 (:65-73, called at :359)
+      vadd(t, uy1, uy0);
+      vmul(u, qy0, uy0);
+      vmul(gy1, qy1, uy1);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) gy1[k] = t[k] > 0 ? u[k] : gy1[k];
+      // compute_rmg_gx (:35-43)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) t[k] = uy0[k] + (k < 3 ? uy0[k + 1] : uyE0);
+      vmul(u, t, c_h);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) gx[k] = t[k] > 0 ? qx0[k] : qx1[k];
+      vmul(gx, gx, u);
+      // compute_rmg_fx (:56-63): qx * ux of the cell or of its west neighbour
+      vmul(u, qx0, ux0);
+      const float pqW = qxW0 * uxW0;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        // compute_rmg_fy (:45-54): ux at the cell and its north neighbour
-        const float uh = (ux0[k] + ux1[k]) * .5f;
-        fy[k] = (ux0[k] + ux1[k] > 0) ? qy0[k] * uh : (k < 3 ? qy0[k + 1] : qyE0) * uh;
-        // compute_rmg_gy for row r+1 (:65-73, called at :359)
-        gy1[k] = (uy1[k] + uy0[k] > 0) ? qy0[k] * uy0[k] : qy1[k] * uy1[k];
-        // compute_rmg_gx (:35-43)
-        const float ue = k < 3 ? uy0[k + 1] : uyE0;
-        const float vh = (uy0[k] + ue) * .5f;
-        gx[k] = (uy0[k] + ue > 0) ? qx0[k] * vh : qx1[k] * vh;
-        // compute_rmg_fx (:56-63)
         const float uw = k > 0 ? ux0[k - 1] : uxW0;
-        const float qw = k > 0 ? qx0[k - 1] : qxW0;
-        fx[k] = (uw + ux0[k] > 0) ? qw * uw : qx0[k] * ux0[k];
+        fx[k] = (uw + ux0[k] > 0) ? (k > 0 ? u[k - 1] : pqW) : u[k];
       }
       const float fyW = __shfl_up_sync(0xffffffffu, fy[3], 1);
       const float fxE = __shfl_down_sync(0xffffffffu, fx[0], 1);
 
       const bool hold_y = (r == 0 || r == H - 2);
-      // face depths and the discharge magnitudes the friction factor uses (:83-92, :110-119)
+      // face depths and the mean cross discharges of the friction factor (:83-92, :110-119)
       float ax0[4], ax1[4], ay0[4], ay1[4], uyx[4], uxy[4];
-      bool movex[4], movey[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) t[k] = h0[k] + (k < 3 ? h0[k + 1] : hE0);
+      vmul(ax0, t, c_h);
+      vadd(t, h0, h1);
+      vmul(ay0, t, c_h);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        ax0[k] = fmaxf(0.f, (h0[k] + (k < 3 ? h0[k + 1] : hE0)) * .5f);
+        ax0[k] = fmaxf(0.f, ax0[k]);
         ax1[k] = fmaxf(ax0[k], kDH);
-        ay0[k] = fmaxf(0.f, (h0[k] + h1[k]) * .5f);
+        ay0[k] = fmaxf(0.f, ay0[k]);
         ay1[k] = fmaxf(ay0[k], kDH);
-        uyx[k] = (qy0[k] + (k < 3 ? qy0[k + 1] : qyE0) + qyS[k] + (k < 3 ? qyS[k + 1] : qySE)) * 0.25f;
-        uxy[k] = (qx0[k] + qx1[k] + (k > 0 ? qx0[k - 1] : qxW0) + (k > 0 ? qx1[k - 1] : qxW1)) * 0.25f;
-        movex[k] = !((qx0[k] == 0.f) & (uyx[k] == 0.f));
-        movey[k] = !((uxy[k] == 0.f) & (qy0[k] == 0.f));
       }
-      float rx[4], ry[4];  // friction factors, 0 where the discharges vanish (:93, :120)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float fxk = friction(fric[k], qx0[k], uyx[k], ax1[k]);
-        const float fyk = friction(fric[k], uxy[k], qy0[k], ay1[k]);
-        rx[k] = movex[k] ? fxk : 0.f;
-        ry[k] = movey[k] ? fyk : 0.f;
+      for (int k = 0; k < 4; ++k) t[k] = qy0[k] + (k < 3 ? qy0[k + 1] : qyE0);
+      vadd(t, t, qyS);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) t[k] = t[k] + (k < 3 ? qyS[k + 1] : qySE);
+      vmul(uyx, t, c_q);
+      vadd(t, qx0, qx1);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) t[k] = (t[k] + (k > 0 ? qx0[k - 1] : qxW0)) + (k > 0 ? qx1[k - 1] : qxW1);
+      vmul(uxy, t, c_q);
+      // friction factors fric * sqrt(ux^2 + uy^2) * (1 / a1)^2.33 (:91-94, :118-121), 0 where both
+      // discharges vanish (then the square sum is 0 and the product is 0 for every finite fric)
+      float rx[4], ry[4];
+      {
+        float mx[4], my[4];
+        vmul(t, uyx, uyx);
+        vfma(mx, qx0, qx0, t);
+        vmul(t, qy0, qy0);
+        vfma(my, uxy, uxy, t);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          t[k] = sqrtf(mx[k]);
+          u[k] = powf(1.f / ax1[k], 2.33f);
+        }
+        vmul(rx, fric, t);
+        vmul(rx, rx, u);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          t[k] = sqrtf(my[k]);
+          u[k] = powf(1.f / ay1[k], 2.33f);
+        }
+        vmul(ry, fric, t);
+        vmul(ry, ry, u);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          rx[k] = (mx[k] == 0.f) ? 0.f : rx[k];
+          ry[k] = (my[k] == 0.f) ? 0.f : ry[k];
+        }
       }
+      // compute_rmg_qx / compute_rmg_qy (:75-127): the same expression trees; 0.5 G h^2 as
+      // nhh = (-0.5 G h) h = -(0.5 G h h)
       float qx2[4], qy2[4];
+      {
+        float nch[4], nhh[4], dsum[4];
+        vmul(nch, h0, c_nhg);
+        vmul(nhh, nch, h0);
+        const float nchE = -kHG * hE0;
+        // x: -dfx - dgx - dhx + dhg
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float fq = upd_qx(k < 3 ? fx[k + 1] : fxE, fx[k], gx[k], gxS[k], dt, dx_inv, rx[k], ax0[k], h0[k],
-                                k < 3 ? h0[k + 1] : hE0, k < 3 ? s0[k + 1] : sE0, s0[k], qx0[k], lim0[k],
-                                k < 3 ? lim0[k + 1] : limE0);
-        const float gq = upd_qy(fy[k], k > 0 ? fy[k - 1] : fyW, gy0[k], gy1[k], dt, dx_inv, ry[k], ay0[k], h0[k],
-                                h1[k], s1[k], s0[k], qy0[k], lim0[k], lim1[k]);
-        qx2[k] = holdX[k] ? qx0[k] : fq;  // boundary-face holds (:373-376)
-        qy2[k] = hold_y ? qy0[k] : gq;
+        for (int k = 0; k < 4; ++k) t[k] = (k < 3 ? fx[k + 1] : fxE) - fx[k];
+        vmul(dsum, t, c_ndxi);                  // -dfx
+        vsub(t, gx, gxS);                       // (gx_i - gx_south)
+        vfma(dsum, t, c_ndxi, dsum);            // - dgx
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          t[k] = fmaf(-(k < 3 ? nch[k + 1] : nchE), k < 3 ? h0[k + 1] : hE0, nhh[k]);  // 0.5G hE hE - 0.5G h h
+        }
+        vfma(dsum, t, c_ndxi, dsum);            // - dhx
+#pragma unroll
+        for (int k = 0; k < 4; ++k) u[k] = s0[k] - (k < 3 ? s0[k + 1] : sE0);  // -s_east + s_i
+        vmul(t, ax0, c_g);
+        vmul(t, t, u);
+        vfma(dsum, t, c_dxi, dsum);             // + dhg
+        vfma(dsum, c_dt, dsum, qx0);            // qx + dt * (...)
+        vadd(t, c_one, rx);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) qx2[k] = dsum[k] / t[k];
+        vadd(qx2, qx2, c_zero);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          float q = fminf(qx2[k], lim0[k]);
+          q = fmaxf(q, -(k < 3 ? lim0[k + 1] : limE0));
+          qx2[k] = holdX[k] ? qx0[k] : q;  // boundary-face holds (:373-376)
+        }
+        // y: -dgy - dfy - dhy + dhg
+        vsub(t, gy1, gy0);
+        vmul(dsum, t, c_ndxi);                  // -dgy
+#pragma unroll
+        for (int k = 0; k < 4; ++k) t[k] = fy[k] - (k > 0 ? fy[k - 1] : fyW);
+        vfma(dsum, t, c_ndxi, dsum);            // - dfy
+        vmul(u, h1, c_hg);
+        vfma(t, u, h1, nhh);                    // 0.5G hN hN - 0.5G h h
+        vfma(dsum, t, c_ndxi, dsum);            // - dhy
+        vsub(u, s0, s1);
+        vmul(t, ay0, c_g);
+        vmul(t, t, u);
+        vfma(dsum, t, c_dxi, dsum);             // + dhg
+        vfma(dsum, c_dt, dsum, qy0);            // qy + dt * (...)
+        vadd(t, c_one, ry);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) qy2[k] = dsum[k] / t[k];
+        vadd(qy2, qy2, c_zero);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          float q = fminf(qy2[k], lim0[k]);
+          q = fmaxf(q, -lim1[k]);
+          qy2[k] = hold_y ? qy0[k] : q;
+        }
       }
       const float qx2W = __shfl_up_sync(0xffffffffu, qx2[3], 1);
 
@@ -538,18 +667,29 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
         const int mH = (store_row && r >= 1 && r <= H - 2) ? (colHm & validm) : 0;
         const int mQX = (store_row && r >= 2 && r <= H - 3) ? (colQXm & validm) : 0;
         const int mQY = (store_row && r >= 1 && r <= H - 3) ? (colQYm & validm) : 0;
+        // continuity (:381): h - dt * dx_inv * ((qx_i - qx_W) + (qy_i - qy_S))
         float h2[4];
 #pragma unroll
+        for (int k = 0; k < 4; ++k) t[k] = qx2[k] - (k > 0 ? qx2[k - 1] : qx2W);
+        vsub(u, qy2, qy2S);
+        vadd(t, t, u);
+        vfma(h2, c_ndtdx, t, h0);
+        // CFL of wet stored cells (:392-396): dx / (sqrt(G h') + max |u|), velocities of the old state
+        vmul(t, c_g, h2);
+#pragma unroll
         for (int k = 0; k < 4; ++k) {
-          h2[k] = h0[k] - dt * dx_inv * ((qx2[k] - (k > 0 ? qx2[k - 1] : qx2W)) + (qy2[k] - qy2S[k]));
+          const float uw = k > 0 ? ux0[k - 1] : uxW0;
+          u[k] = fmaxf(fabsf(uy0[k]), fmaxf(fabsf(uyS[k]), fmaxf(fabsf(ux0[k]), fabsf(uw))));
+          t[k] = sqrtf(t[k]);
+        }
+        vadd(t, t, u);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
           const bool wk = (mH >> k) & 1;
           expacc = max(expacc, __float_as_uint(h2[k]) & 0x7f800000u);  // all-ones exponent: NaN/Inf
-          // CFL of wet stored cells (:392-396), velocities of the old state
-          const float uw = k > 0 ? ux0[k - 1] : uxW0;
-          const float umax = fmaxf(fabsf(uy0[k]), fmaxf(fabsf(uyS[k]), fmaxf(fabsf(ux0[k]), fabsf(uw))));
-          const float dtc = dx / (sqrtf(kG * h2[k]) + umax);
+          const float dtc = dx / t[k];
           cfl = fminf(cfl, (wk && h2[k] > kEPS) ? dtc : 1.0f);
-          nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & inmask[k];
+          nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & 0x7fffffffu;
         }
         const size_t row_off = (size_t)r * (size_t)pitch + (size_t)c;
         if (mH == 15) {
@@ -590,13 +730,24 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
         }
         // per-tile wet flag for the next plan, flushed at the tile's last row
         if (store_row && ((r + 1) % FIP_TILE_ROWS == 0 || r + 1 == rb)) {
-          if (__any_sync(0xffffffffu, nzacc != 0u) && lane == 0) nzs[s * a.n_ty + r / FIP_TILE_ROWS] = 1;
+          // halo lanes hold the neighbouring strips' cells; columns beyond W only occur in the last
+          // strip, whose tiles are always computed anyway
+          if (__any_sync(0xffffffffu, out_lane && nzacc != 0u) && lane == 0) nzs[s * a.n_ty + r / FIP_TILE_ROWS] = 1;
           nzacc = 0u;
         }
       }
 
       nzacc = store_row_flag(r, ra) ? nzacc : 0u;  // the extra row below a run is no part of a tile
-      release_row(r - 1);
+      release_slot(iS);
+      // next row: slots advance by one
+      iS = i0;
+      i0 = i1;
+      i1 = i2;
+      ++i2;
+      if (i2 == (uint32_t)kNSlot) {
+        i2 = 0;
+        ph2 ^= 1u;
+      }
       // travel north (:408-433)
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
@@ -613,9 +764,9 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
       limE0 = __shfl_down_sync(0xffffffffu, lim0[0], 1);
     }
     if (!ok) break;
-    release_row(rb - 1);
-    release_row(rb);
-    release_row(rb + 1);
+    release_slot(iS);  // rows rb-1, rb, rb+1
+    release_slot(i0);
+    release_slot(i1);
     seq += (uint32_t)(rb - ra + 4);
   }
 
@@ -776,7 +927,7 @@ int rmg_step_grid(int device) {
 template <bool KVAR>
 static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t stream) {
   constexpr int NF = KVAR ? 5 : 4;
-  constexpr int kNSlot = KVAR ? FIP_NSLOT_KVAR : FIP_NSLOT_UNIFORM;
+  constexpr int kNSlot = KVAR ? kNSlotKvar : kNSlotUniform;
   const int smem = kNSlot * NF * kFieldBytes + 1024;
   static bool configured = false;
   if (!configured) {
