@@ -9,8 +9,8 @@
 //     sqrtf/powf/division are the same approximations);
 //   * the domain is cut into tiles of 480 columns x 32 rows. A CTA has four consumer warps
 //     (each thread owns 4 adjacent columns, a warp 128 columns of which the 120 inner ones are
-//     stored) and one producer warp that streams rows of h/qx/qy/terrain/kSt into a ring of 7
-//     rows (8 without kSt) in shared memory with TMA (cp.async.bulk.tensor, no multicast).
+//     stored) and one producer warp that streams rows of h/qx/qy/terrain/kSt into a ring of 6
+//     rows (7 without kSt) in shared memory with TMA (cp.async.bulk.tensor, no multicast).
 //     Consumers march north row by row over the staged rows r-1 .. r+2, exchange east/west
 //     neighbours with warp shuffles and do the arithmetic on FP32x2 pairs of columns;
 //   * work = the concatenation of the active tiles' rows (strip-major), split evenly over the
@@ -37,9 +37,9 @@ namespace {
 constexpr float kDH = 0.01f;         // src/kernels.cu:23
 constexpr float kEPS = 10e-7f;       // src/kernels.cu:24 (EPS_TROCKEN)
 constexpr float kG = 9.81f;          // src/simdata.h:358
-constexpr int kNSlotKvar = 7;
-constexpr int kNSlotUniform = 8;
-constexpr int kNSlotMax = 8;  // ring depth in rows: 7 with the kSt field (3 CTAs per SM fit), else 8
+constexpr int kNSlotKvar = 6;
+constexpr int kNSlotUniform = 7;
+constexpr int kNSlotMax = 8;  // ring depth in rows: 6 with the kSt field, else 7 (leaves L1 room beside 3 CTAs)
 constexpr int kMinCtas = 3;  // resident CTAs per SM (128 registers per thread)
 constexpr int kFieldBytes = FIP_SMEM_COLS * 4;  // 2048 B per staged row of one field
 constexpr int kConsumerWarps = 4;
@@ -361,7 +361,9 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
   constexpr float kHG = 0.5f * kG;  // the reference's 0.5f * kG prefix, folded at compile time
   const float2 c_hg = make_float2(kHG, kHG), c_nhg = make_float2(-kHG, -kHG);
 
-  float cfl = 1.0f;
+  // CFL: dx / (sqrt(G h') + max |u|) is monotone in its denominator, so the minimum over the cells
+  // is dx over the largest denominator; the division happens once per warp
+  float den_max = 0.0f;
   unsigned expacc = 0u;  // largest exponent field of a computed depth
   uint32_t seq = 0;
   Walk w = walk0;
@@ -687,8 +689,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
         for (int k = 0; k < 4; ++k) {
           const bool wk = (mH >> k) & 1;
           expacc = max(expacc, __float_as_uint(h2[k]) & 0x7f800000u);  // all-ones exponent: NaN/Inf
-          const float dtc = dx / t[k];
-          cfl = fminf(cfl, (wk && h2[k] > kEPS) ? dtc : 1.0f);
+          den_max = fmaxf(den_max, (wk && h2[k] > kEPS) ? t[k] : 0.0f);
           nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & 0x7fffffffu;
         }
         const size_t row_off = (size_t)r * (size_t)pitch + (size_t)c;
@@ -791,11 +792,13 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
     }
   }
 
-  // CFL minimum: warp reduction, one atomicMin per warp on the float bits (all positive)
+  // CFL minimum (capped at 1, the reference's initial value): warp reduction of the largest
+  // denominator, one atomicMin per warp on the float bits (all positive)
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) cfl = fminf(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+  for (int off = 16; off > 0; off >>= 1) den_max = fmaxf(den_max, __shfl_xor_sync(0xffffffffu, den_max, off));
   const bool any_bad = __any_sync(0xffffffffu, expacc == 0x7f800000u);
   if (lane == 0) {
+    const float cfl = den_max > 0.0f ? fminf(1.0f, dx / den_max) : 1.0f;
     if (cfl < 1.0f) atomicMin(&ctl->cfl_bits[it & 1], __float_as_uint(cfl));
     if (any_bad) ctl->nonfinite = 1;
   }
