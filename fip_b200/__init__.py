@@ -17,9 +17,9 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import FIELDS, FipError, FipInfo, FipOptions, bc_program, config_json, validate
+from ._lib import FIELDS, EnsembleInfo, EnsembleTune, FipError, FipInfo, FipOptions, bc_program, config_json, validate
 
-__all__ = ["Simulation", "FipError", "validate", "config_json", "bc_program", "FIELDS"]
+__all__ = ["Simulation", "Ensemble", "FipError", "validate", "config_json", "bc_program", "FIELDS"]
 
 
 class Simulation:
@@ -109,6 +109,91 @@ class Simulation:
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
             _lib.lib().fip_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Ensemble:
+    """Many scenarios stepped together on one GPU (a fip_ensemble): one stencil launch and one
+    post-kernel launch per ensemble step over every member still short of its target duration.
+    Each member computes what a Simulation of its own parameter file computes."""
+
+    def __init__(self, yaml_paths, device: int = 0, use_graphs: bool = True, all_tiles: bool = False,
+                 stop_on_nonfinite: bool = False):
+        L = _lib.lib()
+        opt = FipOptions()
+        L.fip_default_options(ctypes.byref(opt))
+        opt.device = device
+        opt.use_graphs = int(use_graphs)
+        opt.all_tiles = int(all_tiles)
+        opt.stop_on_nonfinite = int(stop_on_nonfinite)
+        opt.quiet = 1
+        paths = [os.fspath(p).encode() for p in yaml_paths]
+        arr = (ctypes.c_char_p * len(paths))(*paths)
+        h = ctypes.c_void_p()
+        _lib.check(L.fip_ensemble_init(arr, len(paths), ctypes.byref(opt), ctypes.byref(h)))
+        self._h = h
+        self.n = len(paths)
+        self.shapes = []
+        for m in range(self.n):
+            cfg = config_json(os.fspath(yaml_paths[m]))
+            self.shapes.append((int(cfg["H"]), int(cfg["W"])))
+
+    def step(self, n: int = 1) -> None:
+        _lib.check(_lib.lib().fip_ensemble_step(self._h, int(n)))
+
+    def run(self) -> None:
+        _lib.check(_lib.lib().fip_ensemble_run(self._h))
+
+    def step_timed(self, n: int) -> float:
+        """n ensemble steps timed on the device: total ms."""
+        t = ctypes.c_float()
+        _lib.check(_lib.lib().fip_ensemble_step_timed(self._h, int(n), ctypes.byref(t)))
+        return t.value
+
+    def autotune(self, steps_per_shape: int = 20):
+        """Times real steps in each tile shape and keeps the fastest: list of dicts per shape."""
+        res = (EnsembleTune * 16)()
+        n = ctypes.c_int()
+        _lib.check(_lib.lib().fip_ensemble_autotune(self._h, int(steps_per_shape), res, 16, ctypes.byref(n)))
+        return [{"consumer_warps": r.consumer_warps, "tile_cols": r.tile_cols, "tile_rows": r.tile_rows,
+                 "steps": r.steps, "ms_per_step": r.ms_per_step} for r in res[:n.value]]
+
+    def set_shape(self, consumer_warps: int, tile_rows: int) -> None:
+        _lib.check(_lib.lib().fip_ensemble_set_shape(self._h, int(consumer_warps), int(tile_rows)))
+
+    def field(self, member: int, name: str = "h") -> np.ndarray:
+        H, W = self.shapes[member]
+        out = np.empty((H, W), np.float32)
+        _lib.check(_lib.lib().fip_ensemble_get_field(self._h, int(member), FIELDS[name],
+                                                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def time(self, member: int):
+        d, dt, it = ctypes.c_double(), ctypes.c_float(), ctypes.c_int()
+        _lib.check(_lib.lib().fip_ensemble_time(self._h, int(member), ctypes.byref(d), ctypes.byref(dt),
+                                                ctypes.byref(it)))
+        return d.value, dt.value, it.value
+
+    def info(self) -> EnsembleInfo:
+        inf = EnsembleInfo()
+        _lib.check(_lib.lib().fip_ensemble_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().fip_ensemble_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __enter__(self):

@@ -26,7 +26,10 @@ FIELDS = {"h": 0, "qx": 1, "qy": 2, "hmax": 3, "h_prev": 4, "qx_prev": 5, "qy_pr
 # every symbol include/fip.h declares
 EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_run", "fip_save", "fip_save_current",
            "fip_sample", "fip_volume", "fip_get_field", "fip_set_field", "fip_time", "fip_info", "fip_profile_steps", "fip_step_timed", "fip_destroy", "fip_rmg_step_noalloc",
-           "fip_last_error", "fip_validate", "fip_config_json", "fip_bc_program")
+           "fip_last_error", "fip_validate", "fip_config_json", "fip_bc_program",
+           "fip_ensemble_init", "fip_ensemble_step", "fip_ensemble_run", "fip_ensemble_autotune", "fip_ensemble_set_shape",
+           "fip_ensemble_step_timed", "fip_ensemble_get_field", "fip_ensemble_time", "fip_ensemble_info",
+           "fip_ensemble_destroy")
 
 
 class FipOptions(ctypes.Structure):
@@ -38,6 +41,19 @@ class FipInfo(ctypes.Structure):
     _fields_ = [("W", ctypes.c_int), ("H", ctypes.c_int), ("pitch", ctypes.c_int), ("n_tiles", ctypes.c_int),
                 ("active_tiles", ctypes.c_int), ("iteration", ctypes.c_int), ("duration", ctypes.c_double),
                 ("dt", ctypes.c_float), ("last_cfl", ctypes.c_float), ("nonfinite", ctypes.c_int)]
+
+
+class EnsembleTune(ctypes.Structure):
+    _fields_ = [("consumer_warps", ctypes.c_int), ("tile_cols", ctypes.c_int), ("tile_rows", ctypes.c_int),
+                ("steps", ctypes.c_int), ("ms_per_step", ctypes.c_float)]
+
+
+class EnsembleInfo(ctypes.Structure):
+    _fields_ = [("n_members", ctypes.c_int), ("active_members", ctypes.c_int), ("cells", ctypes.c_longlong),
+                ("packed_W", ctypes.c_int), ("packed_rows", ctypes.c_int), ("pitch", ctypes.c_int),
+                ("consumer_warps", ctypes.c_int), ("tile_cols", ctypes.c_int), ("tile_rows", ctypes.c_int),
+                ("n_tiles", ctypes.c_int), ("active_tiles", ctypes.c_int), ("iteration", ctypes.c_int),
+                ("nonfinite", ctypes.c_int)]
 
 
 class FipError(RuntimeError):
@@ -77,6 +93,18 @@ def lib():
         L.fip_rmg_step_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_float, vp, vp, vp, ip, ip, ip, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_float, vp, vp]
         L.fip_rmg_step_noalloc.restype = ctypes.c_int
+        L.fip_ensemble_init.argtypes = [ctypes.POINTER(ctypes.c_char_p), ip, ctypes.POINTER(FipOptions),
+                                        ctypes.POINTER(vp)]
+        L.fip_ensemble_step.argtypes = [vp, ip]
+        L.fip_ensemble_run.argtypes = [vp]
+        L.fip_ensemble_autotune.argtypes = [vp, ip, ctypes.POINTER(EnsembleTune), ip, ctypes.POINTER(ctypes.c_int)]
+        L.fip_ensemble_set_shape.argtypes = [vp, ip, ip]
+        L.fip_ensemble_step_timed.argtypes = [vp, ip, fp]
+        L.fip_ensemble_get_field.argtypes = [vp, ip, ip, fp]
+        L.fip_ensemble_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double), fp, ctypes.POINTER(ctypes.c_int)]
+        L.fip_ensemble_info.argtypes = [vp, ctypes.POINTER(EnsembleInfo)]
+        L.fip_ensemble_destroy.argtypes = [vp]
+        L.fip_ensemble_destroy.restype = None
         L.fip_destroy.argtypes = [vp]
         L.fip_destroy.restype = None
         L.fip_last_error.restype = ctypes.c_char_p
@@ -85,7 +113,9 @@ def lib():
         L.fip_bc_program.argtypes = [ctypes.c_char_p, ip, ip, ctypes.c_char_p, ip]
         for name in ("fip_init", "fip_init_ex", "fip_step", "fip_run", "fip_save", "fip_save_current", "fip_sample",
                      "fip_volume", "fip_get_field", "fip_set_field", "fip_time", "fip_info", "fip_profile_steps", "fip_step_timed", "fip_validate",
-                     "fip_config_json", "fip_bc_program"):
+                     "fip_config_json", "fip_bc_program", "fip_ensemble_init", "fip_ensemble_step", "fip_ensemble_run",
+                     "fip_ensemble_autotune", "fip_ensemble_set_shape", "fip_ensemble_step_timed",
+                     "fip_ensemble_get_field", "fip_ensemble_time", "fip_ensemble_info"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

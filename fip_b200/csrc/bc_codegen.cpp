@@ -192,6 +192,172 @@ const char kPostKernelTail[] = R"FIPSRC(
 }
 )FIPSRC";
 
+// Ensemble counterparts of fip_plan / fip_advance. A member whose target duration is reached
+// drops out of the plan (its tiles are no longer computed) and keeps the buffer of its last
+// state in final_parity; the others step on together with their own dt.
+const char kEnsLib[] = R"FIPSRC(
+__device__ __forceinline__ int fip_ens_member_of(const FipEnsPostArgs& a, int t) {
+  int lo = 0, hi = a.n_members;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a.members[mid].tile_base <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ void fip_ens_plan(const FipEnsPostArgs& a, const FipCtl* ctl, int k, int chunk, bool step_mode) {
+  __shared__ int s_act[FIP_POST_THREADS / 32];
+  __shared__ int s_inact[FIP_POST_THREADS / 32];
+  const int t = chunk * FIP_PLAN_CHUNK + threadIdx.x;
+  const unsigned char* nzc = a.nz[k & 1];
+  unsigned char* nzp = a.nz[(k + 1) & 1];
+  const bool valid = t < a.n_tiles;
+  bool act = false;
+  if (valid) {
+    const int m = fip_ens_member_of(a, t);
+    const FipEnsMember M = a.members[m];
+    const FipEnsCtl* mc = a.mctl + m;
+    // runs in the next step: active now and, after a step, still short of its target
+    bool runs = mc->active != 0;
+    if (step_mode && runs) runs = (mc->duration + (double)mc->dt) < mc->target;
+    const int local = t - M.tile_base;
+    const int sx = local / M.n_ty, ty = local - sx * M.n_ty;
+    act = a.sticky[t] || nzp[t] || ctl->force_all;
+    for (int ds = -1; ds <= 1 && !act; ++ds) {
+      const int s2 = sx + ds;
+      if (s2 < 0 || s2 >= M.n_sx) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y2 = ty + dy;
+        if (y2 < 0 || y2 >= M.n_ty) continue;
+        if (nzc[M.tile_base + s2 * M.n_ty + y2]) { act = true; break; }
+      }
+    }
+    act = act && runs;
+    nzp[t] = 0;
+  }
+  const unsigned ba = __ballot_sync(0xffffffffu, valid && act);
+  const unsigned bi = __ballot_sync(0xffffffffu, valid && !act);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { s_act[warp] = __popc(ba); s_inact[warp] = __popc(bi); }
+  __syncthreads();
+  int base = 0, ibase = 0, total = 0;
+  for (int w = 0; w < FIP_POST_THREADS / 32; ++w) {
+    if (w < warp) { base += s_act[w]; ibase += s_inact[w]; }
+    total += s_act[w];
+  }
+  int* list = a.list[(k + 1) & 1] + chunk * FIP_PLAN_CHUNK;
+  const unsigned below = (1u << lane) - 1u;
+  if (valid && act) list[base + __popc(ba & below)] = t;
+  if (valid && !act) list[FIP_PLAN_CHUNK - 1 - (ibase + __popc(bi & below))] = t;
+  if (threadIdx.x == 0) a.chunk_cnt[(k + 1) & 1][chunk] = total;
+}
+
+// Whole block: every running member advances its time (double += float) and dt controller
+// (controlTimestep, src/main.cpp:25-43) from its own CFL minimum; the ensemble's iteration and
+// buffer parity advance once.
+__device__ void fip_ens_advance(const FipEnsPostArgs& a) {
+  __shared__ int s_running;
+  FipCtl* ctl = a.ctl;
+  const int k = ctl->iteration;
+  const int new_parity = ctl->parity ^ 1;
+  if (threadIdx.x == 0) s_running = 0;
+  __syncthreads();
+  int running = 0;
+  for (int m = threadIdx.x; m < a.n_members; m += blockDim.x) {
+    FipEnsCtl* mc = a.mctl + m;
+    if (!mc->active) continue;
+    const float dt = mc->dt;
+    const float cfl = __uint_as_float(mc->cfl_bits[k & 1]);
+    mc->cfl_bits[k & 1] = __float_as_uint(1.0f);
+    mc->last_cfl = cfl;
+    const double dur = mc->duration + (double)dt;
+    mc->duration = dur;
+    mc->iteration += 1;
+    if (mc->variable_dt) {
+      float min_cfl = 42.0f;
+      if (cfl < min_cfl) min_cfl = cfl;
+      const float target = min_cfl * .5f;
+      const float dc = 0.001f;
+      float d = dt;
+      if (d < target && target - d > dc) d *= 1.001f;
+      else if (d > target && d - target > dc) d *= 0.99f;
+      mc->dt = d;
+    }
+    if (dur >= mc->target) {
+      mc->active = 0;
+      mc->final_parity = new_parity;
+    } else {
+      ++running;
+    }
+  }
+  if (running) atomicAdd(&s_running, running);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ctl->iteration = k + 1;
+    ctl->parity = new_parity;
+    int reason = 0;
+    if (--ctl->steps_left <= 0) reason |= FIP_STOP_BUDGET;
+    if (s_running == 0) reason |= FIP_STOP_TARGET;
+    if (ctl->nonfinite && ctl->stop_on_nonfinite) reason |= FIP_STOP_NONFINITE;
+    if (ctl->error) reason |= FIP_STOP_ERROR;
+    ctl->post_done = 0u;
+    if (reason) {
+      ctl->stop_reason = reason;
+      __threadfence();
+      ctl->stop = 1;
+    }
+  }
+}
+)FIPSRC";
+
+const char kEnsKernelHead[] = R"FIPSRC(
+extern "C" __global__ void __launch_bounds__(FIP_POST_THREADS) fip_ens_post(const FipEnsPostArgs a) {
+  __shared__ float s_buf[4096];
+  __shared__ float s_val[2];
+  __shared__ int s_last;
+  FipCtl* ctl = a.ctl;
+  if (*((volatile int*)&ctl->stop)) return;
+  const bool step_mode = (a.mode == FIP_POST_MODE_STEP);
+  const int k = step_mode ? ctl->iteration : ctl->iteration - 1;
+  if (blockIdx.x < a.n_members) {
+    const int m = blockIdx.x;
+    const FipEnsCtl* mc = a.mctl + m;
+    if (a.mode != FIP_POST_MODE_PLAN && mc->active) {
+      const int cur = step_mode ? (ctl->parity ^ 1) : ctl->parity;
+      const double t_d = step_mode ? mc->duration + (double)mc->dt : mc->duration;
+      const float t = __double2float_rn(t_d);  // TimeSeries::interp(float time)
+      const long long pitch = a.pitch;
+      const long long rbase = (long long)a.members[m].row_off * pitch;
+      float* h = a.h[cur] + rbase;
+      float* qx = a.qx[cur] + rbase;
+      float* qy = a.qy[cur] + rbase;
+      const float* sohle = a.sohle + rbase;
+      (void)t; (void)h; (void)qx; (void)qy; (void)sohle; (void)s_buf; (void)s_val; (void)pitch;
+      switch (m) {
+)FIPSRC";
+
+const char kEnsKernelTail[] = R"FIPSRC(
+      default: break;
+      }
+    }
+  } else {
+    fip_ens_plan(a, ctl, k, blockIdx.x - a.n_members, step_mode);
+  }
+  if (!step_mode) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(&ctl->post_done, 1u);
+    s_last = (prev == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    fip_ens_advance(a);
+  }
+}
+)FIPSRC";
+
 std::string flit(float v) {  // exact float literal
   uint32_t b;
   std::memcpy(&b, &v, 4);
@@ -235,7 +401,10 @@ SideExpr side_expr(BcSide side) {
 // thread first loads the operands of 4 cells and then stores them, which lets the loads of the
 // 4 cells overlap. The arithmetic is the reference's fragment (src_type_*, src/bc_kernel_gen.cpp:
 // 75-137) verbatim in effect: no multiply-add pairs, IEEE sqrtf, so the same rounding.
-void emit_cells(std::ostream& o, const BoundaryCondition& bc, bool staggered) {
+// sign_pitch > 0: the outflow sign of a top/bottom open boundary is +-sign_pitch (the row pitch of
+// the scenario's own buffers) instead of the index difference (packed ensemble rows have a wider
+// pitch than the member's own buffers).
+void emit_cells(std::ostream& o, const BoundaryCondition& bc, bool staggered, long long sign_pitch = 0) {
   const SideExpr e = side_expr(bc.side);
   const char* qi = staggered ? "stg[u]" : "ci[u]";
   o << "      float* const q = " << e.q << ";\n      float* const q_lateral = " << e.q_lateral << ";\n";
@@ -299,8 +468,11 @@ void emit_cells(std::ostream& o, const BoundaryCondition& bc, bool staggered) {
     case BcType::open:
       o << "          const float ah_neighbor = L0[u];\n"
            "          const float z_neighbor = ah_neighbor + L1[u];\n"
-           "          const float sign = (float)(ci[u] - nbr[u]);\n"
-           "          if (ah_neighbor > 0.f) {\n"
+        << (sign_pitch > 0 && (bc.side == BcSide::top || bc.side == BcSide::bottom)
+                ? std::string("          const float sign = (float)(") + (bc.side == BcSide::top ? "" : "-") +
+                      std::to_string(sign_pitch) + "LL);\n"
+                : std::string("          const float sign = (float)(ci[u] - nbr[u]);\n"))
+        << "          if (ah_neighbor > 0.f) {\n"
            "            q["
         << qi
         << "] = sign * sqrtf(FIP_G * ah_neighbor) * ah_neighbor;\n"
@@ -334,6 +506,45 @@ SeriesLayout layout_series(const Config& cfg) {
   return s;
 }
 
+namespace {
+
+// zval / qval of condition i for the current step (getZ / getQ, src/boundary_condition.cpp:50-77):
+// constants for fixed values, device-side interpolation and wet sum for time series. `pitch` is
+// the row pitch the generated code indexes with, `series_base` the offset of this scenario's
+// tables in a.series, `dx_expr` the expression of the cell size.
+void emit_condition_values(std::ostream& o, const Config& cfg, const SeriesLayout& ser, size_t i, long long pitch,
+                           long long series_base, const std::string& dx_expr) {
+  const BoundaryCondition& bc = cfg.bcs[i];
+  if (!bc.is_series) {
+    o << "      const float zval = " << flit(cfg.const_z(bc)) << ";\n";
+    o << "      const float qval = " << flit(cfg.const_q(bc)) << ";\n";
+    return;
+  }
+  if (ser.z_off[i] >= 0)
+    o << "      const float zval = fip_interp_block(a.series + " << series_base + ser.z_off[i] << "L, " << ser.z_n[i]
+      << ", t);\n";
+  else
+    o << "      const float zval = 0.f;\n";
+  if (bc.type == BcType::q) {
+    long long base = 0, inc = 1;
+    switch (bc.side) {
+      case BcSide::left: base = 0; inc = pitch; break;
+      case BcSide::right: base = (long long)cfg.W - 1; inc = pitch; break;
+      case BcSide::top: base = (long long)(cfg.H - 1) * pitch; inc = 1; break;
+      case BcSide::bottom: base = 0; inc = 1; break;
+    }
+    o << "      const float wsum = fip_sum_depths(sohle, " << base << "LL, " << inc << "LL, " << bc.from << ", " << bc.to
+      << ", zval, " << dx_expr << ", s_buf);\n";
+    o << "      if (threadIdx.x == 0) s_val[1] = wsum;\n      __syncthreads();\n";
+    o << "      const float qval = __fdiv_rn(fip_interp_block(a.series + " << series_base + ser.q_off[i] << "L, "
+      << ser.q_n[i] << ", t), s_val[1]);\n";
+  } else {
+    o << "      const float qval = 0.f;\n";
+  }
+}
+
+}  // namespace
+
 std::string post_kernel_source(const Config& cfg, const SeriesLayout& ser, int pitch) {
   std::ostringstream o;
   o << "// generated by fip_b200 from " << cfg.yaml_path << "\n";
@@ -342,37 +553,37 @@ std::string post_kernel_source(const Config& cfg, const SeriesLayout& ser, int p
     const BoundaryCondition& bc = cfg.bcs[i];
     o << "    {  // condition " << i << ": " << side_name(bc.side) << " " << type_name(bc.type) << ", cells "
       << bc.from << ".." << bc.to << (bc.is_series ? ", time series" : "") << "\n";
-    if (!bc.is_series) {
-      o << "      const float zval = " << flit(cfg.const_z(bc)) << ";\n";
-      o << "      const float qval = " << flit(cfg.const_q(bc)) << ";\n";
-    } else {
-      // getZ / getQ of BoundaryConditionTimeseries (src/boundary_condition.cpp:56-77)
-      if (ser.z_off[i] >= 0)
-        o << "      const float zval = fip_interp_block(a.series + " << ser.z_off[i] << "L, " << ser.z_n[i] << ", t);\n";
-      else
-        o << "      const float zval = 0.f;\n";
-      if (bc.type == BcType::q) {
-        long long base = 0, inc = 1;
-        switch (bc.side) {
-          case BcSide::left: base = 0; inc = pitch; break;
-          case BcSide::right: base = (long long)cfg.W - 1; inc = pitch; break;
-          case BcSide::top: base = (long long)(cfg.H - 1) * pitch; inc = 1; break;
-          case BcSide::bottom: base = 0; inc = 1; break;
-        }
-        o << "      const float wsum = fip_sum_depths(sohle, " << base << "LL, " << inc << "LL, " << bc.from << ", "
-          << bc.to << ", zval, a.dx, s_buf);\n";
-        o << "      if (threadIdx.x == 0) s_val[1] = wsum;\n      __syncthreads();\n";
-        o << "      const float qval = __fdiv_rn(fip_interp_block(a.series + " << ser.q_off[i] << "L, " << ser.q_n[i]
-          << ", t), s_val[1]);\n";
-      } else {
-      o << "      const float qval = 0.f;\n";
-      }
-    }
+    emit_condition_values(o, cfg, ser, i, pitch, 0, "a.dx");
     o << "      (void)zval; (void)qval;\n";
     emit_cells(o, bc, cfg.staggered());
     o << "      __syncthreads();\n    }\n";
   }
   o << kPostKernelTail;
+  return o.str();
+}
+
+std::string ensemble_post_kernel_source(const std::vector<const Config*>& cfgs, const std::vector<SeriesLayout>& sers,
+                                        const std::vector<long long>& series_base,
+                                        const std::vector<FipEnsMember>& members, int pitch) {
+  std::ostringstream o;
+  o << "// generated by fip_b200 for an ensemble of " << cfgs.size() << " scenarios\n";
+  o << kCtlHeader << kPostLib << kEnsLib << kEnsKernelHead;
+  for (size_t m = 0; m < cfgs.size(); ++m) {
+    const Config& cfg = *cfgs[m];
+    o << "      case " << m << ": {  // " << cfg.yaml_path << "\n";
+    o << "        const long long W = " << cfg.W << "LL, H = " << cfg.H << "LL;\n        (void)W; (void)H;\n";
+    for (size_t i = 0; i < cfg.bcs.size(); ++i) {
+      const BoundaryCondition& bc = cfg.bcs[i];
+      o << "    {  // condition " << i << ": " << side_name(bc.side) << " " << type_name(bc.type) << ", cells "
+        << bc.from << ".." << bc.to << (bc.is_series ? ", time series" : "") << "\n";
+      emit_condition_values(o, cfg, sers[m], i, pitch, series_base[m], flit(cfg.dx));
+      o << "      (void)zval; (void)qval;\n";
+      emit_cells(o, bc, cfg.staggered(), members[m].pitch_ref);
+      o << "      __syncthreads();\n    }\n";
+    }
+    o << "      } break;\n";
+  }
+  o << kEnsKernelTail;
   return o.str();
 }
 
@@ -402,7 +613,7 @@ int compile_post_kernel(const std::string& source, std::string* cubin, std::stri
   return 0;
 }
 
-int build_post_kernel(const std::string& source, PostKernel* out, std::string* err) {
+int build_post_kernel(const std::string& source, PostKernel* out, std::string* err, const char* entry) {
   std::string cubin;
   out->source = source;
   if (compile_post_kernel(source, &cubin, &out->log, err)) return -1;
@@ -412,9 +623,9 @@ int build_post_kernel(const std::string& source, PostKernel* out, std::string* e
     *err = drv::message(cr, "cuModuleLoadData");
     return -1;
   }
-  cr = drv::ModuleGetFunction(&out->fn, out->module, "fip_post");
+  cr = drv::ModuleGetFunction(&out->fn, out->module, entry);
   if (cr != CUDA_SUCCESS) {
-    *err = "cuModuleGetFunction(fip_post) failed";
+    *err = std::string("cuModuleGetFunction(") + entry + ") failed";
     return -1;
   }
   return 0;

@@ -27,6 +27,14 @@ SeriesLayout layout_series(const Config& cfg);
 // scales its outflow by idx - idx_neighbor = +-pitch, src/bc_kernel_gen.cpp:122, :132).
 std::string post_kernel_source(const Config& cfg, const SeriesLayout& ser, int pitch);
 
+// Post kernel of a packed ensemble (fip_ens_post): block m < members applies member m's
+// conditions (its rows start at members[m].row_off of the packed buffers with row pitch `pitch`),
+// the other blocks plan the next step's tiles, the last block advances every member.
+// series_base[m] is the offset of member m's tables in the concatenated series array.
+std::string ensemble_post_kernel_source(const std::vector<const Config*>& cfgs, const std::vector<SeriesLayout>& sers,
+                                        const std::vector<long long>& series_base,
+                                        const std::vector<FipEnsMember>& members, int pitch);
+
 struct PostKernel {
   CUmodule module = nullptr;
   CUfunction fn = nullptr;
@@ -37,7 +45,8 @@ struct PostKernel {
 int compile_post_kernel(const std::string& source, std::string* cubin, std::string* log, std::string* err);
 
 // compile_post_kernel + cuModuleLoadData. Returns 0 or a message in *err.
-int build_post_kernel(const std::string& source, PostKernel* out, std::string* err);
+int build_post_kernel(const std::string& source, PostKernel* out, std::string* err,
+                      const char* entry = "fip_post");
 void destroy_post_kernel(PostKernel* k);
 
 }  // namespace fip

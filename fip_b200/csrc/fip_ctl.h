@@ -80,4 +80,50 @@ struct FipPostArgs {
   int pad_;
 };
 
+// ---- batched ensembles: many scenarios stacked in one set of pitched buffers ----
+// Member m occupies rows [row_off, row_off + H) of every packed field (columns [0, W)); the rows
+// between members and the columns right of W stay zero, so each member reads exactly what its
+// own buffers would hold. Its tiles are [tile_base, tile_base + n_sx * n_ty) of the ensemble's
+// concatenated tile list, strip-major like a single scenario.
+#define FIP_ENS_MAX_MEMBERS 256
+
+struct FipEnsMember {
+  int tile_base, n_sx, n_ty;
+  int W, H, row_off;
+  float dx, kst_fixed, no_value;
+  int pitch_ref;  // row pitch (elements) of the member's own buffers: scales top/bottom open outflow
+};
+
+// Per-member state of the ensemble's step loop (the members' counterparts of FipCtl's scalars).
+struct FipEnsCtl {
+  double duration;  // simulated time after the member's last step
+  double target;    // the member's target duration
+  float dt;         // dt of the member's next step
+  float last_cfl;
+  int iteration;    // steps the member ran
+  int active;       // 1 while duration < target: the member steps with the ensemble
+  int variable_dt;
+  int final_parity; // buffer holding the member's state once it stopped
+  unsigned int cfl_bits[2];
+  int pad_[2];
+};
+
+// Argument block of the generated ensemble post kernel.
+struct FipEnsPostArgs {
+  float* h[2];
+  float* qx[2];
+  float* qy[2];
+  const float* sohle;
+  FipCtl* ctl;  // ensemble-wide: stop, parity, iteration, budget, errors
+  FipEnsCtl* mctl;
+  const FipEnsMember* members;
+  const unsigned char* sticky;
+  unsigned char* nz[2];
+  int* list[2];
+  int* chunk_cnt[2];
+  const float* series;
+  int pitch, n_members, n_tiles, n_chunks;
+  int tile_cols, tile_rows, mode, pad_;
+};
+
 #endif  // FIP_CTL_H

@@ -39,7 +39,12 @@ constexpr float kEPS = 10e-7f;       // src/kernels.cu:24 (EPS_TROCKEN)
 constexpr float kG = 9.81f;          // src/simdata.h:358
 constexpr int kNSlotKvar = 6;
 constexpr int kNSlotUniform = 7;
-constexpr int kNSlotMax = 8;  // ring depth in rows: 6 with the kSt field, else 7 (leaves L1 room beside 3 CTAs)
+constexpr int kNSlotMax = 10;  // ring depth in rows: 6 with the kSt field, else 7 (leaves L1 room beside 3 CTAs)
+// two-warp tiles (240 columns, used by ensembles when the autotuner picks them): 5 CTAs per SM,
+// deeper rings in their smaller rows
+constexpr int kNSlotKvar2 = 8;
+constexpr int kNSlotUniform2 = 10;
+constexpr int kMinCtas2 = 5;
 constexpr int kMinCtas = 3;  // resident CTAs per SM (128 registers per thread)
 constexpr int kFieldBytes = FIP_SMEM_COLS * 4;  // 2048 B per staged row of one field
 constexpr int kConsumerWarps = 4;
@@ -61,6 +66,10 @@ struct StepArgs {
   int W, H, pitch;
   int n_sx, n_ty, n_tiles, n_chunks;
   float dx, kst_fixed, no_value;
+  // ensembles only: member table, per-member control, member count, tile rows
+  const FipEnsMember* members;
+  FipEnsCtl* mctl;
+  int n_members, tile_rows;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -179,8 +188,9 @@ __device__ __forceinline__ void vfma(float (&d)[4], float2 a, const float (&b)[4
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
 
+template <int FB = kFieldBytes>
 __device__ __forceinline__ float4 lds4(const unsigned char* slot, int field, int col) {
-  return *reinterpret_cast<const float4*>(slot + field * kFieldBytes + col * 4);
+  return *reinterpret_cast<const float4*>(slot + field * FB + col * 4);
 }
 
 // Walk of a CTA's share of the active-tile row stream: maximal runs of rows that are
@@ -225,21 +235,71 @@ __device__ __forceinline__ bool next_run(Walk& w, const int* list, const int* s_
   return false;
 }
 
-template <bool KVAR>
-__global__ void __launch_bounds__(kThreads, kMinCtas)
+// next_run over an ensemble's concatenated tile list: the member of the run's tiles comes from
+// the members' first tile indices (s_tbase, n_members + 1 entries); rows are the member's own.
+__device__ __forceinline__ bool next_run_ens(Walk& w, const int* list, const int* s_prefix, int n_chunks, int TR,
+                                             const FipEnsMember* mem, const int* s_tbase, int n_members, int* member,
+                                             int* strip, int* ra, int* rb) {
+  while (w.pos < w.end) {
+    long long p = w.pos / TR;
+    const int off = (int)(w.pos - p * TR);
+    int tile = list_entry(list, s_prefix, n_chunks, p);
+    int lo = 0, hi = n_members;  // s_tbase[lo] <= tile < s_tbase[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s_tbase[mid] <= tile) lo = mid;
+      else hi = mid;
+    }
+    const int n_ty = mem[lo].n_ty, H = mem[lo].H;
+    const int local = tile - s_tbase[lo];
+    const int s = local / n_ty;
+    const int ty0 = local - s * n_ty;
+    int ty = ty0;
+    while ((p + 1) * TR < w.end && ty + 1 < n_ty && list_entry(list, s_prefix, n_chunks, p + 1) == tile + 1) {
+      ++p;
+      ++tile;
+      ++ty;
+    }
+    const long long stop = (p + 1) * TR < w.end ? (p + 1) * TR : w.end;
+    const int r_a = ty0 * TR + off;
+    int r_b = ty * TR + (int)(stop - p * TR);
+    w.pos = stop;
+    if (r_b > H) r_b = H;
+    if (r_a >= r_b) continue;
+    *member = lo;
+    *strip = s;
+    *ra = r_a;
+    *rb = r_b;
+    return true;
+  }
+  return false;
+}
+
+// KW consumer warps per CTA (tiles of 120 * KW columns); ENS: the grid is a packed ensemble
+// (member table in the arguments, per-member dt, rows, sizes and CFL slots).
+template <bool KVAR, bool ENS, int KW>
+__global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
     rmg_step_kernel(const __grid_constant__ CUtensorMap tm_h0, const __grid_constant__ CUtensorMap tm_h1,
                     const __grid_constant__ CUtensorMap tm_qx0, const __grid_constant__ CUtensorMap tm_qx1,
                     const __grid_constant__ CUtensorMap tm_qy0, const __grid_constant__ CUtensorMap tm_qy1,
                     const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_k,
                     const StepArgs a) {
   constexpr int NF = KVAR ? 5 : 4;
-  constexpr int kNSlot = KVAR ? kNSlotKvar : kNSlotUniform;
-  constexpr int kSlotBytes = NF * kFieldBytes;
+  constexpr int kNSlot = KW == 4 ? (KVAR ? kNSlotKvar : kNSlotUniform) : (KVAR ? kNSlotKvar2 : kNSlotUniform2);
+  constexpr int kFB = KW * 128 * 4;  // bytes of one staged row of one field
+  constexpr int kSlotBytes = NF * kFB;
+  constexpr int TC = 120 * KW;       // tile columns
+  // staged column of the tile's column 0: lanes read [X0 - 4, X0 + 120 * KW + 4) of the staged
+  // 128 * KW columns (TMA x stays a multiple of 4 floats either way)
+  constexpr int X0 = KW == 2 ? 4 : FIP_SMEM_X0;
+  static_assert(KW == 2 || KW == 4, "tiles of 2 or 4 consumer warps");
+  static_assert(kNSlot <= kNSlotMax, "ring depth");
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t full_bar[kNSlotMax];
   __shared__ __align__(8) uint64_t empty_bar[kNSlotMax];
   __shared__ int s_prefix[kMaxChunks + 1];
   __shared__ int s_hdr[6];
+  __shared__ int s_tbase[ENS ? FIP_ENS_MAX_MEMBERS + 1 : 1];
 
   unsigned char* ring = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
   FipCtl* ctl = a.ctl;
@@ -252,12 +312,16 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
     s_hdr[2] = ctl->iteration;
     s_hdr[3] = __float_as_int(ctl->dt);
     s_hdr[4] = (ctl->hmax_every > 0 && ctl->iteration > 0 && ctl->iteration % ctl->hmax_every == 0) ? 1 : 0;
-    s_hdr[5] = ctl->hmax_full;
+    s_hdr[5] = ENS ? 0 : ctl->hmax_full;  // ensembles fold every tile (force_all) instead
     for (int i = 0; i < kNSlot; ++i) {
       mbar_init(&full_bar[i], 1);
-      mbar_init(&empty_bar[i], kConsumerWarps);
+      mbar_init(&empty_bar[i], KW);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (ENS) {
+    for (int i = tid; i <= a.n_members; i += blockDim.x)
+      s_tbase[i] = i < a.n_members ? a.members[i].tile_base : a.n_tiles;
   }
   if (tid < 32) {  // prefix over the chunk counts of this step's plan
     const int par = ctl->parity;
@@ -280,13 +344,14 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
   const float dt = __int_as_float(s_hdr[3]);
   const bool fold = s_hdr[4] != 0;
   const int* list = a.list[it & 1];
-  const long long total = (long long)s_prefix[a.n_chunks] * FIP_TILE_ROWS;
+  const int TR = ENS ? a.tile_rows : FIP_TILE_ROWS;
+  const long long total = (long long)s_prefix[a.n_chunks] * TR;
   const long long G = gridDim.x;
   Walk walk0;
   walk0.pos = total * blockIdx.x / G;
   walk0.end = total * (blockIdx.x + 1) / G;
 
-  if (warp == kConsumerWarps) {
+  if (warp == KW) {
     // ---------------- producer: one elected thread streams rows with TMA ----------------
     if (lane == 0) {
       const CUtensorMap* th = par ? &tm_h1 : &tm_h0;
@@ -295,9 +360,12 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
       Walk w = walk0;
       uint32_t seq = 0;
       bool ok = true;
-      int s, ra, rb;
-      while (ok && next_run(w, list, s_prefix, a.n_chunks, a.n_ty, a.H, &s, &ra, &rb)) {
-        const int x0 = s * FIP_TILE_COLS - FIP_SMEM_X0;
+      int s, ra, rb, m = 0;
+      while (ok && (ENS ? next_run_ens(w, list, s_prefix, a.n_chunks, TR, a.members, s_tbase, a.n_members, &m, &s,
+                                       &ra, &rb)
+                        : next_run(w, list, s_prefix, a.n_chunks, a.n_ty, a.H, &s, &ra, &rb))) {
+        const int x0 = s * TC - X0;
+        const int y0 = ENS ? a.members[m].row_off : 0;
         for (int j = ra - 2; j <= rb + 1; ++j, ++seq) {
           const uint32_t slot = seq % kNSlot;
           const uint32_t ph = (seq / kNSlot) & 1u;
@@ -308,17 +376,14 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
           }
           unsigned char* dst = ring + slot * kSlotBytes;
           mbar_arrive_expect_tx(&full_bar[slot], kSlotBytes);
-          tma_row(dst + F_H * kFieldBytes, th, x0, j, &full_bar[slot]);
-          tma_row(dst + F_H * kFieldBytes + 1024, th, x0 + 256, j, &full_bar[slot]);
-          tma_row(dst + F_QX * kFieldBytes, tqx, x0, j, &full_bar[slot]);
-          tma_row(dst + F_QX * kFieldBytes + 1024, tqx, x0 + 256, j, &full_bar[slot]);
-          tma_row(dst + F_QY * kFieldBytes, tqy, x0, j, &full_bar[slot]);
-          tma_row(dst + F_QY * kFieldBytes + 1024, tqy, x0 + 256, j, &full_bar[slot]);
-          tma_row(dst + F_S * kFieldBytes, &tm_s, x0, j, &full_bar[slot]);
-          tma_row(dst + F_S * kFieldBytes + 1024, &tm_s, x0 + 256, j, &full_bar[slot]);
-          if (KVAR) {
-            tma_row(dst + F_K * kFieldBytes, &tm_k, x0, j, &full_bar[slot]);
-            tma_row(dst + F_K * kFieldBytes + 1024, &tm_k, x0 + 256, j, &full_bar[slot]);
+          const int y = y0 + j;
+#pragma unroll
+          for (int b = 0; b < KW / 2; ++b) {
+            tma_row(dst + F_H * kFB + 1024 * b, th, x0 + 256 * b, y, &full_bar[slot]);
+            tma_row(dst + F_QX * kFB + 1024 * b, tqx, x0 + 256 * b, y, &full_bar[slot]);
+            tma_row(dst + F_QY * kFB + 1024 * b, tqy, x0 + 256 * b, y, &full_bar[slot]);
+            tma_row(dst + F_S * kFB + 1024 * b, &tm_s, x0 + 256 * b, y, &full_bar[slot]);
+            if (KVAR) tma_row(dst + F_K * kFB + 1024 * b, &tm_k, x0 + 256 * b, y, &full_bar[slot]);
           }
         }
       }
@@ -336,26 +401,34 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
   }
 
   // ---------------- consumers ----------------
-  const float dx = a.dx;
-  const float dx_inv = 1.f / dx;  // in-kernel, as the reference (:276-277)
-  const float dt_inv = 1.f / dt;
-  const float fric_u = dt * kG / (a.kst_fixed * a.kst_fixed);  // uniform kSt: dt * G / (kSt * kSt)
-  const float dtg = dt * kG;                                    // kSt_var: (dt * G) / (kSt * kSt)
-  const int W = a.W, H = a.H, pitch = a.pitch;
-  const float nv = a.no_value;
-  const int scol = FIP_SMEM_X0 - 4 + 120 * warp + 4 * lane;  // staged column of k = 0
+  // per-scenario scalars: fixed for a single grid, set at every run for an ensemble member
+  float dx = a.dx, dtm = dt, kstf = a.kst_fixed, nv = a.no_value;
+  int W = a.W, H = a.H, row0 = 0, tbase = 0, nty = a.n_ty;
+  const int pitch = a.pitch;
+  float dx_inv, dt_inv, fric_u, dtg, dtdx;
+  float2 c_dti, c_dx, c_dxi, c_ndxi, c_dt, c_ndtdx;
+  auto set_scalars = [&]() {
+    dx_inv = 1.f / dx;  // in-kernel, as the reference (:276-277)
+    dt_inv = 1.f / dtm;
+    fric_u = dtm * kG / (kstf * kstf);  // uniform kSt: dt * G / (kSt * kSt)
+    dtg = dtm * kG;                     // kSt_var: (dt * G) / (kSt * kSt)
+    // broadcast operands of the packed arithmetic
+    c_dti = make_float2(dt_inv, dt_inv);
+    c_dx = make_float2(dx, dx);
+    c_dxi = make_float2(dx_inv, dx_inv);
+    c_ndxi = make_float2(-dx_inv, -dx_inv);
+    c_dt = make_float2(dtm, dtm);
+    dtdx = dtm * dx_inv;  // dt * dx_inv of the continuity update (:381), left to right
+    c_ndtdx = make_float2(-dtdx, -dtdx);
+  };
+  set_scalars();
+  const int scol = X0 - 4 + 120 * warp + 4 * lane;  // staged column of k = 0
   const bool out_lane = (lane >= 1 && lane <= 30);
   float* const h_out = a.h[par ^ 1];
   float* const qx_out = a.qx[par ^ 1];
   float* const qy_out = a.qy[par ^ 1];
   const float* const h_in = a.h[par];
   unsigned char* const nzs = a.nz[it & 1];
-  // broadcast operands of the packed arithmetic
-  const float2 c_dti = make_float2(dt_inv, dt_inv), c_dx = make_float2(dx, dx);
-  const float2 c_dxi = make_float2(dx_inv, dx_inv), c_ndxi = make_float2(-dx_inv, -dx_inv);
-  const float2 c_dt = make_float2(dt, dt);
-  const float dtdx = dt * dx_inv;  // dt * dx_inv of the continuity update (:381), left to right
-  const float2 c_ndtdx = make_float2(-dtdx, -dtdx);
   const float2 c_q = make_float2(0.25f, 0.25f), c_h = make_float2(0.5f, 0.5f), c_one = make_float2(1.f, 1.f);
   const float2 c_g = make_float2(kG, kG), c_zero = make_float2(0.f, 0.f);
   constexpr float kHG = 0.5f * kG;  // the reference's 0.5f * kG prefix, folded at compile time
@@ -367,9 +440,23 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
   unsigned expacc = 0u;  // largest exponent field of a computed depth
   uint32_t seq = 0;
   Walk w = walk0;
-  int s, ra, rb;
-  while (next_run(w, list, s_prefix, a.n_chunks, a.n_ty, H, &s, &ra, &rb)) {
-    const int c = s * FIP_TILE_COLS - 4 + 120 * warp + 4 * lane;  // global column of k = 0
+  int s, ra, rb, m = 0;
+  while (ENS ? next_run_ens(w, list, s_prefix, a.n_chunks, TR, a.members, s_tbase, a.n_members, &m, &s, &ra, &rb)
+             : next_run(w, list, s_prefix, a.n_chunks, a.n_ty, H, &s, &ra, &rb)) {
+    if (ENS) {
+      const FipEnsMember& M = a.members[m];
+      W = M.W;
+      H = M.H;
+      row0 = M.row_off;
+      tbase = M.tile_base;
+      nty = M.n_ty;
+      dx = M.dx;
+      kstf = M.kst_fixed;
+      nv = M.no_value;
+      dtm = a.mctl[m].dt;
+      set_scalars();
+    }
+    const int c = s * TC - 4 + 120 * warp + 4 * lane;  // global column of k = 0
     // 4-bit column masks of the cell sets the reference's kernel writes (src/kernels.cu:383-406)
     int colHm = 0, colQXm = 0, colQYm = 0, colInm = 0;
     bool holdX[4];
@@ -411,12 +498,12 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
       const unsigned char* slA = ring + iS * kSlotBytes;
       const unsigned char* slB = ring + i0 * kSlotBytes;
       const unsigned char* slC = ring + i1 * kSlotBytes;
-      const float4 vhs = lds4(slA, F_H, scol);
-      const float4 vqys = lds4(slA, F_QY, scol);
-      const float4 vh0 = lds4(slB, F_H, scol);
-      const float4 vqx0 = lds4(slB, F_QX, scol);
-      const float4 vqy0 = lds4(slB, F_QY, scol);
-      const float4 vh1 = lds4(slC, F_H, scol);
+      const float4 vhs = lds4<kFB>(slA, F_H, scol);
+      const float4 vqys = lds4<kFB>(slA, F_QY, scol);
+      const float4 vh0 = lds4<kFB>(slB, F_H, scol);
+      const float4 vqx0 = lds4<kFB>(slB, F_QX, scol);
+      const float4 vqy0 = lds4<kFB>(slB, F_QY, scol);
+      const float4 vh1 = lds4<kFB>(slC, F_H, scol);
       const float hs[4] = {vhs.x, vhs.y, vhs.z, vhs.w};
       const float qyS[4] = {vqys.x, vqys.y, vqys.z, vqys.w};
       const float h0[4] = {vh0.x, vh0.y, vh0.z, vh0.w};
@@ -462,28 +549,28 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
       const unsigned char* sl2 = ring + i2 * kSlotBytes;
       float h2r[4], qx1[4], qy1[4], s1[4], fric[4], qyS[4], s0[4], h0[4], h1[4], qx0[4], qy0[4];
       {
-        const float4 vqs = lds4(slS, F_QY, scol);
-        const float4 vs0 = lds4(sl0, F_S, scol);
-        const float4 vh0 = lds4(sl0, F_H, scol);
-        const float4 vqx0 = lds4(sl0, F_QX, scol);
-        const float4 vqy0 = lds4(sl0, F_QY, scol);
-        const float4 vh1 = lds4(sl1, F_H, scol);
+        const float4 vqs = lds4<kFB>(slS, F_QY, scol);
+        const float4 vs0 = lds4<kFB>(sl0, F_S, scol);
+        const float4 vh0 = lds4<kFB>(sl0, F_H, scol);
+        const float4 vqx0 = lds4<kFB>(sl0, F_QX, scol);
+        const float4 vqy0 = lds4<kFB>(sl0, F_QY, scol);
+        const float4 vh1 = lds4<kFB>(sl1, F_H, scol);
         qyS[0] = vqs.x; qyS[1] = vqs.y; qyS[2] = vqs.z; qyS[3] = vqs.w;
         s0[0] = vs0.x; s0[1] = vs0.y; s0[2] = vs0.z; s0[3] = vs0.w;
         h0[0] = vh0.x; h0[1] = vh0.y; h0[2] = vh0.z; h0[3] = vh0.w;
         qx0[0] = vqx0.x; qx0[1] = vqx0.y; qx0[2] = vqx0.z; qx0[3] = vqx0.w;
         qy0[0] = vqy0.x; qy0[1] = vqy0.y; qy0[2] = vqy0.z; qy0[3] = vqy0.w;
         h1[0] = vh1.x; h1[1] = vh1.y; h1[2] = vh1.z; h1[3] = vh1.w;
-        const float4 v2 = lds4(sl2, F_H, scol);
-        const float4 vqx = lds4(sl1, F_QX, scol);
-        const float4 vqy = lds4(sl1, F_QY, scol);
-        const float4 vs = lds4(sl1, F_S, scol);
+        const float4 v2 = lds4<kFB>(sl2, F_H, scol);
+        const float4 vqx = lds4<kFB>(sl1, F_QX, scol);
+        const float4 vqy = lds4<kFB>(sl1, F_QY, scol);
+        const float4 vs = lds4<kFB>(sl1, F_S, scol);
         h2r[0] = v2.x; h2r[1] = v2.y; h2r[2] = v2.z; h2r[3] = v2.w;
         qx1[0] = vqx.x; qx1[1] = vqx.y; qx1[2] = vqx.z; qx1[3] = vqx.w;
         qy1[0] = vqy.x; qy1[1] = vqy.y; qy1[2] = vqy.z; qy1[3] = vqy.w;
         s1[0] = vs.x; s1[1] = vs.y; s1[2] = vs.z; s1[3] = vs.w;
         if (KVAR) {
-          const float4 vk = lds4(sl0, F_K, scol);
+          const float4 vk = lds4<kFB>(sl0, F_K, scol);
           float kk[4] = {vk.x, vk.y, vk.z, vk.w};
           vmul(kk, kk, kk);
 #pragma unroll
@@ -692,7 +779,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
           den_max = fmaxf(den_max, (wk && h2[k] > kEPS) ? t[k] : 0.0f);
           nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & 0x7fffffffu;
         }
-        const size_t row_off = (size_t)r * (size_t)pitch + (size_t)c;
+        const size_t row_off = (size_t)(r + row0) * (size_t)pitch + (size_t)c;
         if (mH == 15) {
           *reinterpret_cast<float4*>(h_out + row_off) = make_float4(h2[0], h2[1], h2[2], h2[3]);
         } else {
@@ -730,10 +817,10 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
           }
         }
         // per-tile wet flag for the next plan, flushed at the tile's last row
-        if (store_row && ((r + 1) % FIP_TILE_ROWS == 0 || r + 1 == rb)) {
+        if (store_row && ((r + 1) % TR == 0 || r + 1 == rb)) {
           // halo lanes hold the neighbouring strips' cells; columns beyond W only occur in the last
           // strip, whose tiles are always computed anyway
-          if (__any_sync(0xffffffffu, out_lane && nzacc != 0u) && lane == 0) nzs[s * a.n_ty + r / FIP_TILE_ROWS] = 1;
+          if (__any_sync(0xffffffffu, out_lane && nzacc != 0u) && lane == 0) nzs[tbase + s * nty + r / TR] = 1;
           nzacc = 0u;
         }
       }
@@ -769,20 +856,30 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
     release_slot(i0);
     release_slot(i1);
     seq += (uint32_t)(rb - ra + 4);
+    if (ENS) {  // this member's CFL minimum: warp reduction, one atomicMin per warp and run
+      float dm = den_max;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) dm = fmaxf(dm, __shfl_xor_sync(0xffffffffu, dm, off));
+      if (lane == 0 && dm > 0.0f) {
+        const float cfl = fminf(1.0f, dx / dm);
+        if (cfl < 1.0f) atomicMin(&a.mctl[m].cfl_bits[it & 1], __float_as_uint(cfl));
+      }
+      den_max = 0.0f;
+    }
   }
 
   // inactive tiles still fold hmax when the initial state had negative depths
   if (fold && s_hdr[5]) {
-    const int ctid = tid;  // 0..127
+    const int ctid = tid;  // consumer thread
     for (int ch = 0; ch < a.n_chunks; ++ch) {
       const int in_chunk = min(FIP_PLAN_CHUNK, a.n_tiles - ch * FIP_PLAN_CHUNK);
       const int n_inact = in_chunk - (s_prefix[ch + 1] - s_prefix[ch]);
       for (int i = blockIdx.x; i < n_inact; i += gridDim.x) {
         const int tile = list[ch * FIP_PLAN_CHUNK + FIP_PLAN_CHUNK - 1 - i];
         const int st = tile / a.n_ty, ty = tile - st * a.n_ty;
-        const int c0 = st * FIP_TILE_COLS, r0 = ty * FIP_TILE_ROWS;
-        for (int e = ctid; e < FIP_TILE_COLS * FIP_TILE_ROWS; e += kConsumerWarps * 32) {
-          const int rr = r0 + e / FIP_TILE_COLS, cc = c0 + e % FIP_TILE_COLS;
+        const int c0 = st * TC, r0 = ty * TR;
+        for (int e = ctid; e < TC * TR; e += KW * 32) {
+          const int rr = r0 + e / TC, cc = c0 + e % TC;
           if (rr < H && cc < W) {
             const size_t o = (size_t)rr * pitch + cc;
             a.hmax[o] = fmaxf(a.hmax[o], h_in[o]);
@@ -804,17 +901,21 @@ __global__ void __launch_bounds__(kThreads, kMinCtas)
   }
 }
 
+// Per tile of a tile_cols x tile_rows grid: sticky flag and whether buffer (h, qx, qy) has a
+// nonzero cell (into nz0 and nz1). With or_into set, the nonzero flag is OR-ed into or_into[t]
+// instead and nothing else is written.
 __global__ void init_tiles_kernel(const float* h, const float* qx, const float* qy, const float* sohle, int W, int H,
-                                  int pitch, float no_value, int n_ty, int n_tiles, unsigned char* sticky,
-                                  unsigned char* nz0, unsigned char* nz1) {
+                                  int pitch, float no_value, int n_ty, int n_tiles, int tile_cols, int tile_rows,
+                                  unsigned char* or_into, unsigned char* sticky, unsigned char* nz0,
+                                  unsigned char* nz1) {
   const int t = blockIdx.x;
   if (t >= n_tiles) return;
   const int s = t / n_ty, ty = t - s * n_ty;
-  const int c0 = s * FIP_TILE_COLS, r0 = ty * FIP_TILE_ROWS;
-  const int c1 = min(c0 + FIP_TILE_COLS, W), r1 = min(r0 + FIP_TILE_ROWS, H);
+  const int c0 = s * tile_cols, r0 = ty * tile_rows;
+  const int c1 = min(c0 + tile_cols, W), r1 = min(r0 + tile_rows, H);
   int nz = 0, st = 0;
-  for (int e = threadIdx.x; e < FIP_TILE_COLS * FIP_TILE_ROWS; e += blockDim.x) {
-    const int r = r0 + e / FIP_TILE_COLS, c = c0 + e % FIP_TILE_COLS;
+  for (int e = threadIdx.x; e < tile_cols * tile_rows; e += blockDim.x) {
+    const int r = r0 + e / tile_cols, c = c0 + e % tile_cols;
     if (r < r1 && c < c1) {
       const size_t o = (size_t)r * pitch + c;
       const bool nzc = (h[o] != 0.f) || (qx[o] != 0.f) || (qy[o] != 0.f);
@@ -827,6 +928,10 @@ __global__ void init_tiles_kernel(const float* h, const float* qx, const float* 
   if (r0 < 4 || r1 > H - 4 || c0 < 4 || c1 > W - 4) st = 1;
   nz = __syncthreads_or(nz);
   st = __syncthreads_or(st);
+  if (or_into) {
+    if (threadIdx.x == 0 && nz) or_into[t] = 1;
+    return;
+  }
   if (threadIdx.x == 0) {
     sticky[t] = (unsigned char)st;
     nz0[t] = (unsigned char)nz;
@@ -927,14 +1032,15 @@ int rmg_step_grid(int device) {
   return kMinCtas * sms;
 }
 
-template <bool KVAR>
+template <bool KVAR, bool ENS, int KW>
 static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t stream) {
   constexpr int NF = KVAR ? 5 : 4;
-  constexpr int kNSlot = KVAR ? kNSlotKvar : kNSlotUniform;
-  const int smem = kNSlot * NF * kFieldBytes + 1024;
+  constexpr int kNSlot = KW == 4 ? (KVAR ? kNSlotKvar : kNSlotUniform) : (KVAR ? kNSlotKvar2 : kNSlotUniform2);
+  const int smem = kNSlot * NF * KW * 128 * 4 + 1024;
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(rmg_step_kernel<KVAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(rmg_step_kernel<KVAR, ENS, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
@@ -959,19 +1065,52 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
   a.dx = st.dx;
   a.kst_fixed = st.kst_fixed;
   a.no_value = st.no_value;
-  rmg_step_kernel<KVAR><<<grid, kThreads, smem, stream>>>(st.tm_h[0], st.tm_h[1], st.tm_qx[0], st.tm_qx[1],
-                                                          st.tm_qy[0], st.tm_qy[1], st.tm_sohle, st.tm_kst, a);
+  a.members = st.members;
+  a.mctl = st.mctl;
+  a.n_members = st.n_members;
+  a.tile_rows = st.tile_rows;
+  rmg_step_kernel<KVAR, ENS, KW><<<grid, (KW + 1) * 32, smem, stream>>>(
+      st.tm_h[0], st.tm_h[1], st.tm_qx[0], st.tm_qx[1], st.tm_qy[0], st.tm_qy[1], st.tm_sohle, st.tm_kst, a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t stream) {
   if (st.n_chunks > kMaxChunks) return cudaErrorInvalidValue;
-  return st.kst ? launch_step_t<true>(st, grid, stream) : launch_step_t<false>(st, grid, stream);
+  if (!st.members) return st.kst ? launch_step_t<true, false, 4>(st, grid, stream) : launch_step_t<false, false, 4>(st, grid, stream);
+  if (st.n_members > FIP_ENS_MAX_MEMBERS || st.tile_rows < 4) return cudaErrorInvalidValue;
+  if (st.kw == 4)
+    return st.kst ? launch_step_t<true, true, 4>(st, grid, stream) : launch_step_t<false, true, 4>(st, grid, stream);
+  if (st.kw == 2)
+    return st.kst ? launch_step_t<true, true, 2>(st, grid, stream) : launch_step_t<false, true, 2>(st, grid, stream);
+  return cudaErrorInvalidValue;
+}
+
+int rmg_step_grid_kw(int device, int kw) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return (kw == 2 ? kMinCtas2 : kMinCtas) * sms;
 }
 
 cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t stream) {
-  init_tiles_kernel<<<st.n_tiles, 256, 0, stream>>>(st.h[parity], st.qx[parity], st.qy[parity], st.sohle, st.W, st.H, st.pitch,
-                                                    st.no_value, st.n_ty, st.n_tiles, st.sticky, st.nz[0], st.nz[1]);
+  init_tiles_kernel<<<st.n_tiles, 256, 0, stream>>>(st.h[parity], st.qx[parity], st.qy[parity], st.sohle, st.W, st.H,
+                                                    st.pitch, st.no_value, st.n_ty, st.n_tiles, FIP_TILE_COLS,
+                                                    FIP_TILE_ROWS, nullptr, st.sticky, st.nz[0], st.nz[1]);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_tiles_region(const float* h, const float* qx, const float* qy, const float* h_other,
+                                     const float* qx_other, const float* qy_other, const float* sohle, int W, int H,
+                                     int pitch, float no_value, int tile_cols, int tile_rows, unsigned char* sticky,
+                                     unsigned char* nz_cur, unsigned char* nz_prev, cudaStream_t stream) {
+  const int n_sx = (W + tile_cols - 1) / tile_cols, n_ty = (H + tile_rows - 1) / tile_rows;
+  init_tiles_kernel<<<n_sx * n_ty, 256, 0, stream>>>(h, qx, qy, sohle, W, H, pitch, no_value, n_ty, n_sx * n_ty,
+                                                     tile_cols, tile_rows, nullptr, sticky, nz_cur, nz_prev);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !h_other) return e;
+  // the other buffer becomes the next step's output: a tile must be computed while it is nonzero
+  init_tiles_kernel<<<n_sx * n_ty, 256, 0, stream>>>(h_other, qx_other, qy_other, sohle, W, H, pitch, no_value, n_ty,
+                                                     n_sx * n_ty, tile_cols, tile_rows, nz_prev, nullptr, nullptr,
+                                                     nullptr);
   return cudaGetLastError();
 }
 

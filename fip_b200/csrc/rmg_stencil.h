@@ -26,6 +26,12 @@ struct StencilState {
   int n_sx, n_ty, n_tiles, n_chunks;
   float dx, kst_fixed, no_value;
   CUtensorMap tm_h[2], tm_qx[2], tm_qy[2], tm_sohle, tm_kst;
+  // packed ensembles (members != nullptr): member table, per-member control, tile shape
+  const FipEnsMember* members = nullptr;
+  FipEnsCtl* mctl = nullptr;
+  int n_members = 0;
+  int tile_rows = FIP_TILE_ROWS;
+  int kw = 4;  // consumer warps per CTA: tiles of 120 * kw columns
 };
 
 // Geometry of the tile grid for a W x H domain.
@@ -39,6 +45,18 @@ cudaError_t launch_rmg_step(const StencilState& st, int grid_ctas, cudaStream_t 
 
 // Per-tile sticky flags and the nonzero flags of state buffer `parity` (into both nz slots).
 cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t stream);
+
+// The same for one region of a packed ensemble (pointers at the member's first row, flags at its
+// first tile) with an explicit tile shape. nz_cur gets the flags of (h, qx, qy); nz_prev those
+// of (h, qx, qy) OR of the other ping-pong buffer when h_other is given, so that a tile whose
+// output buffer still holds water is computed.
+cudaError_t launch_init_tiles_region(const float* h, const float* qx, const float* qy, const float* h_other,
+                                     const float* qx_other, const float* qy_other, const float* sohle, int W, int H,
+                                     int pitch, float no_value, int tile_cols, int tile_rows, unsigned char* sticky,
+                                     unsigned char* nz_cur, unsigned char* nz_prev, cudaStream_t stream);
+
+// CTAs the step kernel runs with for tiles of kw consumer warps (3 per SM for 4 warps, 5 for 2).
+int rmg_step_grid_kw(int device, int kw);
 
 // hmax = max(hmax, h[parity]) over the whole grid (the reference's flood_plains_kernel).
 cudaError_t launch_hmax_fold(const StencilState& st, int parity, cudaStream_t stream);

@@ -264,3 +264,78 @@ def scenario1(outdir: str, W: int = 5667, H: int = 6500, dx: float = 3.0, dt: fl
     return Scenario(ypath, W, H, z, kst_var=kst,
                     info={"inflow_rows": (r0, r1 - 1), "no_data": no_data,
                           "series": (ts, qs, zs)})
+
+
+def ensemble_member(outdir: str, W: int, H: int, seed: int, kst: float = 30.0, q_peak: float = 1000.0,
+                    t_peak: float = 3 * 3600.0, duration: float = 6 * 3600.0, dx: float = 3.0, dt: float = 0.5,
+                    name: str | None = None, right: str = "open", bottom: str | None = None) -> Scenario:
+    """One member of the batched ensemble: fBm valley (Hurst 0.8) draining to the right edge with
+    a meandering channel, uniform kSt, dry start, variable dt, left q inflow over the channel
+    entry with a triangular hydrograph 0 -> q_peak (at t_peak) -> q_peak / 5 (at the end) plus the
+    stage series the q type requires, right edge `right`, top and bottom closed unless `bottom`
+    names a type."""
+    os.makedirs(outdir, exist_ok=True)
+    name = name or f"member{seed}"
+    scale = min(W, H) / 1024.0
+    y = np.arange(H, dtype=np.float32)[:, None]
+    x = np.arange(W, dtype=np.float32)[None, :]
+    relief = 6.0 * max(scale, 0.25) ** 0.5
+    z = fbm(W, H, 0.8, seed) * relief
+    xs = np.arange(W, dtype=np.float32)
+    yc = H * 0.5 + 0.2 * H * np.sin(2 * np.pi * xs / max(W * 0.7, 16.0))
+    # valley: banks rising away from the channel, the floor falling towards the right edge
+    dist = np.abs(y - yc[None, :])
+    z = z + 0.004 * dx * dist - 0.001 * dx * x
+    half = max(2, int(round(20 * scale)))
+    z = np.where(dist <= half, z - 2.5, z).astype(np.float32)
+    n_in = max(4, min(H - 4, 2 * half + 4))
+    r0 = int(np.clip(int(yc[0]) - n_in // 2, 1, H - n_in - 2))
+    r1 = r0 + n_in
+    bed_in = float(z[r0:r1, 0].min())
+    ts = np.arange(0.0, duration + 600.0, 600.0)
+    qs = np.where(ts <= t_peak, q_peak * ts / max(t_peak, 1.0),
+                  q_peak + (0.2 * q_peak - q_peak) * (ts - t_peak) / max(duration - t_peak, 1.0))
+    qs = np.maximum(qs, 0.0)
+    stage = 0.3 + 2.5 * (qs / max(q_peak, 1e-9)) ** 0.6
+    zs = bed_in + stage
+    tpath = os.path.join(outdir, f"{name}_terrain.bin")
+    write_grid(tpath, z)
+    qpath = os.path.join(outdir, f"{name}_q.csv")
+    zpath = os.path.join(outdir, f"{name}_z.csv")
+    write_series(qpath, ts, qs, header="time;discharge")
+    write_series(zpath, ts, zs, header="time;stage")
+    bcs = [{"side": "left", "type": "q", "q": [qpath, 0, 1], "z": [zpath, 0, 1], "from": r0, "to": r1 - 1},
+           {"side": "right", "type": right}]
+    if bottom:
+        bcs.append({"side": "bottom", "type": bottom})
+    cfg = {
+        "#0": f"seed {seed}: ensemble_member(W={W}, H={H}, kSt={kst:.4g}, q_peak={q_peak:.6g}, t_peak={t_peak:.6g})",
+        "name": os.path.join(outdir, name),
+        "terrain": [tpath, 0],
+        "W": W, "H": H, "dx": dx, "dt": dt,
+        "duration": duration,
+        "kSt": f"{kst:.9g}",
+        "variable_dt": True,
+        "boundary_conditions": bcs,
+    }
+    ypath = os.path.join(outdir, f"{name}.yml")
+    write_yaml(ypath, cfg)
+    return Scenario(ypath, W, H, z, info={"inflow_rows": (r0, r1 - 1), "kst": kst, "q_peak": q_peak,
+                                          "t_peak": t_peak})
+
+
+def ensemble2(outdir: str, n: int = 64, seed: int = 2, size_lo: int = 256, size_hi: int = 2048,
+              duration: float = 6 * 3600.0) -> list:
+    """The batched-ensemble workload: n members with W, H ~ U[size_lo, size_hi], their own fBm
+    seeds, kSt ~ U[20, 45], hydrograph peak ~ U[200, 2000] m3/s at U[1, 8] h, 6 simulated hours."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        W = int(rng.integers(size_lo, size_hi + 1))
+        H = int(rng.integers(size_lo, size_hi + 1))
+        kst = float(rng.uniform(20.0, 45.0))
+        q_peak = float(rng.uniform(200.0, 2000.0))
+        t_peak = float(rng.uniform(1.0, 8.0)) * 3600.0
+        out.append(ensemble_member(outdir, W, H, seed=1000 * seed + m, kst=kst, q_peak=q_peak, t_peak=t_peak,
+                                   duration=duration, name=f"m{m:03d}"))
+    return out

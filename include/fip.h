@@ -169,6 +169,51 @@ int fip_config_json(const char* yaml_path, char* buf, int buflen);
  * source length or a negative error. */
 int fip_bc_program(const char* yaml_path, int pitch, int compile, char* buf, int buflen);
 
+/* ---- Batched ensembles (no counterpart in the reference, which runs one scenario per process,
+ * src/main.cpp:204-263) ----
+ * Many parameter files advanced together: every ensemble step is one stencil launch and one
+ * post-kernel launch over all members still short of their target duration. Each member
+ * computes exactly what fip_init + fip_step compute for its own file (own dt controller,
+ * boundary conditions, flood plains); sampling points and save_state times of the members are
+ * ignored. Members are stacked in one set of device buffers; tile shape is chosen by
+ * fip_ensemble_autotune or fip_ensemble_set_shape. */
+typedef struct fip_ensemble fip_ensemble;
+
+typedef struct {
+  int consumer_warps;  /* 2 or 4: tiles of 240 or 480 columns */
+  int tile_cols, tile_rows;
+  int steps;           /* ensemble steps timed in this shape */
+  float ms_per_step;   /* device time per ensemble step (CUDA events) */
+} fip_ensemble_tune_t;
+
+typedef struct {
+  int n_members, active_members;
+  long long cells;     /* sum of the members' W * H */
+  int packed_W, packed_rows, pitch;
+  int consumer_warps, tile_cols, tile_rows;
+  int n_tiles, active_tiles;  /* tiles of all members / computed by the next step */
+  int iteration;       /* ensemble steps taken */
+  int nonfinite;
+} fip_ensemble_info_t;
+
+int fip_ensemble_init(const char* const* yaml_paths, int n_members, const fip_options* opt, fip_ensemble** out);
+/* n_steps ensemble steps (members that reached their target duration stay as they are). */
+int fip_ensemble_step(fip_ensemble* e, int n_steps);
+/* Until every member reached its target duration. */
+int fip_ensemble_run(fip_ensemble* e);
+/* Times steps_per_shape real ensemble steps in each tile shape (the state advances; results
+ * do not depend on the shape) and keeps the fastest. Fills up to max_results entries. */
+int fip_ensemble_autotune(fip_ensemble* e, int steps_per_shape, fip_ensemble_tune_t* results, int max_results,
+                          int* n_results);
+int fip_ensemble_set_shape(fip_ensemble* e, int consumer_warps, int tile_rows);
+/* n_steps ensemble steps timed with CUDA events on the ensemble's stream. */
+int fip_ensemble_step_timed(fip_ensemble* e, int n_steps, float* total_ms);
+/* Member field (FIP_FIELD_H .. FIP_FIELD_TERRAIN) into a W x H host buffer. */
+int fip_ensemble_get_field(fip_ensemble* e, int member, int field, float* host);
+int fip_ensemble_time(fip_ensemble* e, int member, double* duration, float* dt, int* iteration);
+int fip_ensemble_info(fip_ensemble* e, fip_ensemble_info_t* out);
+void fip_ensemble_destroy(fip_ensemble* e);
+
 /* Message of the last failed call on this thread ("" if none). */
 const char* fip_last_error(void);
 
