@@ -158,6 +158,68 @@ def cpu_baseline(sc, seconds: float, steps_hint: int | None = None):
                       f"{n} steps in {dt:.1f} s, {threads} threads"}, n, dt
 
 
+def ensemble_measure(args, local_rank):
+    """Batched ensemble of 64 scenarios (W, H ~ U[256, 2048], own fBm terrain, kSt ~ U[20, 45],
+    triangular inflow peaking at U[200, 2000] m3/s after U[1, 8] h, variable dt), FP32.
+
+    * batched: one Ensemble, every tile computed, tile shape autotuned, `ens_steps` ensemble
+      steps timed with CUDA events (graphs of 64 steps);
+    * sequential: the same members one at a time as single-scenario runs (the reference runs one
+      scenario per process), every tile computed, `ens_seq_steps` steps each, device time;
+    * flooded: the ensemble with dry-tile skipping after `ens_spinup` steps (whole-ensemble
+      cell updates per second, i.e. every member's every cell, and the active-tile fraction).
+    Speed-up = per-step time of the sequential runs summed over members / batched per-step time.
+    """
+    from fip_b200 import Ensemble, Simulation, synth
+
+    d = os.path.join(tempfile.gettempdir(), f"fip_bench_ens_{os.getpid()}")
+    t0 = time.perf_counter()
+    members = synth.ensemble2(d, n=args.ens_members, seed=2)
+    gen_s = time.perf_counter() - t0
+    paths = [m.yaml_path for m in members]
+    cells = sum(m.W * m.H for m in members)
+    out = {"workload": f"ensemble of {len(paths)} scenarios, W,H ~ U[256,2048], kSt ~ U[20,45], variable dt",
+           "members": len(paths), "cells": cells, "input_gen_s": round(gen_s, 1)}
+    t0 = time.perf_counter()
+    with Ensemble(paths, device=local_rank, all_tiles=True) as e:
+        out["init_s"] = round(time.perf_counter() - t0, 1)
+        e.step(3)
+        tune = e.autotune(steps_per_shape=10)
+        inf = e.info()
+        e.step_timed(8)
+        ms = e.step_timed(args.ens_steps)
+    out["autotune"] = [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} for r in tune]
+    out["shape"] = {"consumer_warps": inf.consumer_warps, "tile_cols": inf.tile_cols, "tile_rows": inf.tile_rows}
+    batched_ms = ms / args.ens_steps
+    out["batched_ms_per_step"] = batched_ms
+    out["batched_cell_updates_per_s"] = cells / (batched_ms / 1e3)
+    out["batched_roofline_frac"] = cells * 28 / (batched_ms / 1e3) / 1e9 / peaks()[0]
+    seq_ms = 0.0
+    t0 = time.perf_counter()
+    for pth in paths:
+        with Simulation(pth, device=local_rank, quiet=True, all_tiles=True) as s:
+            s.step_timed(3)
+            tot, _, _ = s.step_timed(args.ens_seq_steps)
+            seq_ms += tot / args.ens_seq_steps
+    out["sequential_ms_per_step"] = seq_ms
+    out["sequential_wall_s"] = round(time.perf_counter() - t0, 1)
+    out["sequential_cell_updates_per_s"] = cells / (seq_ms / 1e3)
+    out["speedup_batched_vs_sequential"] = seq_ms / batched_ms
+    if args.ens_spinup > 0:
+        with Ensemble(paths, device=local_rank) as e:
+            e.step(args.ens_spinup)
+            e.autotune(steps_per_shape=10)
+            inf = e.info()
+            ms = e.step_timed(args.ens_steps)
+            t_sim = [e.time(m)[0] for m in range(len(paths))]
+        out["flooded"] = {"after_steps": args.ens_spinup, "sim_time_s_median": float(np.median(t_sim)),
+                          "active_tile_fraction": inf.active_tiles / max(inf.n_tiles, 1),
+                          "shape": [inf.consumer_warps, inf.tile_rows],
+                          "ms_per_step": ms / args.ens_steps,
+                          "whole_ensemble_cell_updates_per_s": cells * args.ens_steps / (ms / 1e3)}
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -258,6 +320,12 @@ def run_gpu(args, rank, world, local_rank):
             "bytes_per_launch": cells * BYTES_PER_CELL, "stencil_ms_per_launch": stencil_ms,
             "post_ms_per_launch": post_ms}
     clocks = clk.summary()
+    ens = None
+    if world == 1 and args.ens_members > 0:
+        try:
+            ens = ensemble_measure(args, local_rank)
+        except Exception as exc:  # reported in the line; the headline stands on its own
+            ens = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
         base = None
         if world == 1 and not args.no_cpu_baseline:
@@ -274,7 +342,7 @@ def run_gpu(args, rank, world, local_rank):
                         "d2h_bytes_per_step": 3 * cells * 4,
                         "note": f"each e2e step = upload h,qx,qy from pinned host + {inner} solver steps + download"},
                 "gpu_launches": 2 * args.steps, "roofline": roof, "clocks": clocks,
-                "cpu_baseline": base, "active_tiles": active}
+                "cpu_baseline": base, "active_tiles": active, "ensemble": ens}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -294,6 +362,10 @@ def main():
     ap.add_argument("--e2e-inner", type=int, default=100)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ens-members", type=int, default=64, help="batched-ensemble measurement (0: skip)")
+    ap.add_argument("--ens-steps", type=int, default=200)
+    ap.add_argument("--ens-seq-steps", type=int, default=20)
+    ap.add_argument("--ens-spinup", type=int, default=3000)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
