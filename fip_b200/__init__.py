@@ -105,6 +105,15 @@ class Simulation:
         _lib.check(_lib.lib().fip_step_timed(self._h, int(n), ctypes.byref(t), ctypes.byref(a), ctypes.byref(b)))
         return t.value, a.value, b.value
 
+    # -- exact resume ----------------------------------------------------------------------
+    def checkpoint(self, path: str) -> None:
+        """Writes both ping-pong buffers, hmax and the step state; see restore()."""
+        _lib.check(_lib.lib().fip_checkpoint(self._h, os.fspath(path).encode()))
+
+    def restore(self, path: str) -> None:
+        """Loads a checkpoint of the same scenario; the run continues bit for bit."""
+        _lib.check(_lib.lib().fip_restore(self._h, os.fspath(path).encode()))
+
     # -- lifetime --------------------------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:

@@ -29,7 +29,7 @@ EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_ru
            "fip_last_error", "fip_validate", "fip_config_json", "fip_bc_program",
            "fip_ensemble_init", "fip_ensemble_step", "fip_ensemble_run", "fip_ensemble_autotune", "fip_ensemble_set_shape",
            "fip_ensemble_step_timed", "fip_ensemble_get_field", "fip_ensemble_time", "fip_ensemble_info",
-           "fip_ensemble_destroy")
+           "fip_ensemble_destroy", "fip_checkpoint", "fip_restore")
 
 
 class FipOptions(ctypes.Structure):
@@ -105,6 +105,10 @@ def lib():
         L.fip_ensemble_info.argtypes = [vp, ctypes.POINTER(EnsembleInfo)]
         L.fip_ensemble_destroy.argtypes = [vp]
         L.fip_ensemble_destroy.restype = None
+        L.fip_checkpoint.argtypes = [vp, ctypes.c_char_p]
+        L.fip_restore.argtypes = [vp, ctypes.c_char_p]
+        L.fip_checkpoint.restype = ctypes.c_int
+        L.fip_restore.restype = ctypes.c_int
         L.fip_destroy.argtypes = [vp]
         L.fip_destroy.restype = None
         L.fip_last_error.restype = ctypes.c_char_p

@@ -9,7 +9,9 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
+#include <cstdint>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -545,6 +547,136 @@ int fip_save_current(fip_handle* h, const char* prefix) {
   if (!h) return fail(FIP_ERR_ARG, "null handle");
   return guard([&] {
     h->dump(prefix ? prefix : h->cfg.name, true);
+    return FIP_OK;
+  });
+}
+
+// ---- exact resume ----
+// The reference's only restart path is to feed a save_state dump back as z/qx/qy input files
+// (offset 16): the dump holds depth while the loader reads z as a level (src/main.cpp:189 vs
+// src/simdata.cpp:266-270), the level round trip rounds the depths, and time, dt, iteration,
+// hmax and the ping-pong partner are lost. A checkpoint keeps all of it, so a restored run
+// continues bit for bit.
+namespace {
+
+constexpr char kCkptMagic[8] = {'F', 'I', 'P', 'C', 'K', 'P', 'T', '1'};
+
+struct CkptHeader {
+  char magic[8];
+  uint32_t version, header_bytes;
+  int64_t W, H;
+  uint64_t terrain_hash;  // FNV-1a over the terrain floats: the checkpoint belongs to this scenario
+  double duration, sample_timer;
+  float dt, last_cfl;
+  int32_t iteration, parity, save_pos, started, nonfinite, hmax_full;
+};
+
+uint64_t fnv1a(const void* p, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  uint64_t x = 1469598103934665603ull;
+  for (size_t i = 0; i < n; ++i) x = (x ^ b[i]) * 1099511628211ull;
+  return x;
+}
+
+}  // namespace
+
+int fip_checkpoint(fip_handle* h, const char* path) {
+  if (!h || !path) return fail(FIP_ERR_ARG, "null argument");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(h->stream), "checkpoint");
+    const size_t W = h->cfg.W, H = h->cfg.H;
+    CkptHeader hd;
+    std::memset(&hd, 0, sizeof hd);
+    std::memcpy(hd.magic, kCkptMagic, 8);
+    hd.version = 1;
+    hd.header_bytes = sizeof hd;
+    hd.W = (int64_t)W;
+    hd.H = (int64_t)H;
+    hd.terrain_hash = fnv1a(h->cfg.terrain.data(), W * H * sizeof(float));
+    hd.duration = h->h_ctl->duration;
+    hd.sample_timer = h->sample_timer;
+    hd.dt = h->h_ctl->dt;
+    hd.last_cfl = h->h_ctl->last_cfl;
+    hd.iteration = h->h_ctl->iteration;
+    hd.parity = h->h_ctl->parity;
+    hd.save_pos = (int32_t)h->save_pos;
+    hd.started = h->started ? 1 : 0;
+    hd.nonfinite = h->h_ctl->nonfinite;
+    hd.hmax_full = h->h_ctl->hmax_full;
+    std::ofstream f(path, std::ios::binary);
+    if (!f) throw std::invalid_argument(std::string("IO:cannot open ") + path);
+    f.write(reinterpret_cast<const char*>(&hd), sizeof hd);
+    const int p = hd.parity;
+    const float* src[7] = {h->st.h[p], h->st.qx[p], h->st.qy[p], h->st.h[p ^ 1], h->st.qx[p ^ 1], h->st.qy[p ^ 1],
+                           h->st.hmax};
+    std::vector<float> buf(W * H);
+    for (const float* s : src) {
+      ck(cudaMemcpy2D(buf.data(), W * 4, s, (size_t)h->st.pitch * 4, W * 4, H, cudaMemcpyDeviceToHost), "checkpoint");
+      f.write(reinterpret_cast<const char*>(buf.data()), (std::streamsize)(W * H * sizeof(float)));
+    }
+    if (!f) throw std::invalid_argument(std::string("IO:write failed: ") + path);
+    return FIP_OK;
+  });
+}
+
+int fip_restore(fip_handle* h, const char* path) {
+  if (!h || !path) return fail(FIP_ERR_ARG, "null argument");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t W = h->cfg.W, H = h->cfg.H;
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw std::invalid_argument(std::string("IO:cannot open ") + path);
+    CkptHeader hd;
+    f.read(reinterpret_cast<char*>(&hd), sizeof hd);
+    if (!f || std::memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != 1 || hd.header_bytes != sizeof hd)
+      throw std::invalid_argument(std::string("IO:") + path + " is not a fip_b200 checkpoint");
+    if (hd.W != (int64_t)W || hd.H != (int64_t)H)
+      throw std::invalid_argument(std::string("checkpoint ") + path + " is for a " + std::to_string(hd.W) + " x " +
+                                  std::to_string(hd.H) + " grid");
+    if (hd.terrain_hash != fnv1a(h->cfg.terrain.data(), W * H * sizeof(float)))
+      throw std::invalid_argument(std::string("checkpoint ") + path + " was written for a different terrain");
+    if (hd.parity != 0 && hd.parity != 1) throw std::invalid_argument(std::string("IO:") + path + ": bad parity");
+    const int p = hd.parity;
+    float* dst[7] = {h->st.h[p], h->st.qx[p], h->st.qy[p], h->st.h[p ^ 1], h->st.qx[p ^ 1], h->st.qy[p ^ 1],
+                     h->st.hmax};
+    std::vector<float> buf(W * H);
+    for (float* d : dst) {
+      f.read(reinterpret_cast<char*>(buf.data()), (std::streamsize)(W * H * sizeof(float)));
+      if (!f) throw std::invalid_argument(std::string("IO:") + path + " is truncated");
+      ck(cudaMemcpy2D(d, (size_t)h->st.pitch * 4, buf.data(), W * 4, W * 4, H, cudaMemcpyHostToDevice), "restore");
+    }
+    FipCtl* c = h->h_ctl;
+    c->duration = hd.duration;
+    c->dt = hd.dt;
+    c->last_cfl = hd.last_cfl;
+    c->iteration = hd.iteration;
+    c->parity = p;
+    c->nonfinite = hd.nonfinite;
+    c->hmax_full = hd.hmax_full;
+    c->stop = c->stop_reason = c->error = 0;
+    c->post_done = 0u;
+    const float one = 1.0f;
+    std::memcpy(&c->cfl_bits[0], &one, 4);
+    std::memcpy(&c->cfl_bits[1], &one, 4);
+    h->sample_timer = hd.sample_timer;
+    h->save_pos = (size_t)std::max(0, hd.save_pos);
+    h->started = hd.started != 0;
+    c->next_save = h->save_pos < h->cfg.save_times.size() ? h->cfg.save_times[h->save_pos] : kInf;
+    c->next_sample = (h->started && h->cfg.sampling_interval > 0) ? h->sample_timer : kInf;
+    c->target = kInf;
+    ck(cudaMemcpyAsync(h->d_ctl, c, sizeof(FipCtl), cudaMemcpyHostToDevice, h->stream), "restore");
+    // exact plan of the restored state: a tile is computed when it or a neighbour holds water, or
+    // while the partner buffer (the next step's output) still holds water in it
+    const int k = hd.iteration - 1;
+    ck(fip::launch_init_tiles_region(h->st.h[p], h->st.qx[p], h->st.qy[p], h->st.h[p ^ 1], h->st.qx[p ^ 1],
+                                     h->st.qy[p ^ 1], h->st.sohle, h->st.W, h->st.H, h->st.pitch, h->st.no_value,
+                                     FIP_TILE_COLS, FIP_TILE_ROWS, h->st.sticky, h->st.nz[k & 1], h->st.nz[(k + 1) & 1],
+                                     h->stream),
+       "init_tiles");
+    if (h->started) h->launch_post(FIP_POST_MODE_PLAN);
+    h->replan = false;
+    ck(cudaStreamSynchronize(h->stream), "restore");
     return FIP_OK;
   });
 }

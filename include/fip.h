@@ -123,6 +123,16 @@ int fip_profile_steps(fip_handle* h, int n_steps, float* stencil_ms, float* post
  * these steps (the state advances normally otherwise). No counterpart in the reference. */
 int fip_step_timed(fip_handle* h, int n_steps, float* total_ms, float* stencil_ms, float* post_ms);
 
+/* Exact-resume checkpoint (replaces the reference's restart through save_state dumps fed back as
+ * z/qx/qy inputs with offset 16, src/main.cpp:154-202 and src/simdata.cpp:266-274, which loses
+ * time, dt, hmax and the ping-pong partner and reads the dumped depth as a level). Writes the
+ * current and partner h/qx/qy buffers, hmax, simulated time, dt, iteration, sampling timer and
+ * save_state position to one file. */
+int fip_checkpoint(fip_handle* h, const char* path);
+/* Restores a checkpoint into a handle created from the same parameter file (same grid size and
+ * terrain, checked); the run then continues bit for bit as if it had never stopped. */
+int fip_restore(fip_handle* h, const char* path);
+
 /* Frees every device and host resource of the handle (the reference leaves this to
  * cudaDeviceReset at exit, src/main.cpp:256). */
 void fip_destroy(fip_handle* h);

@@ -1,0 +1,93 @@
+"""Host-side logic of libfip_b200.so, run without a GPU: the C ABI loads and exports every entry
+point include/fip.h declares, parameter files are validated and parsed like the reference's
+loader (src/simdata.cpp:152-310), time series (seconds or %d.%m.%Y %H:%M:%S stamps,
+src/timeseries.cpp:28-84) are read like the reference, and the boundary-condition program is
+generated and compiled by NVRTC for sm_100a. No call here touches a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import pyoracle
+from fip_b200 import FipError, _lib, bc_program, config_json, synth, validate
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = []
+    for hdr in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if hdr.endswith(".h"):
+            with open(os.path.join(ROOT, "include", hdr)) as f:
+                text = re.sub(r"/\*.*?\*/", "", f.read(), flags=re.S)
+            names += re.findall(r"^[A-Za-z_][\w \*]*?\b(fip_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    names = _declared()
+    assert "fip_init" in names and "fip_rmg_step_noalloc" in names and "fip_ensemble_init" in names
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert sorted(_lib.EXPORTS) == names
+
+
+def test_validate_and_parse(tmp_path):
+    sc = synth.scenario1(str(tmp_path), W=64, H=48, seed=2, duration=600.0, name="v")
+    validate(sc.yaml_path)
+    cfg = config_json(sc.yaml_path)
+    assert (cfg["W"], cfg["H"], cfg["dx"]) == (64, 48, 3.0)
+    assert cfg["variable_dt"] and cfg["kst_var"] and cfg["no_data"] == -1.0
+    assert [b["type"] for b in cfg["boundary_conditions"]] == ["q", "open"]
+    bad = tmp_path / "bad.yml"
+    bad.write_text(open(sc.yaml_path).read().replace("W: 64", "W: 65"))
+    with pytest.raises(FipError):  # the terrain file is one row short for W = 65
+        validate(str(bad))
+
+
+def test_defaults_follow_the_reference(tmp_path):
+    """variable_dt defaults to true, kSt to 30, no_data to -9999 (src/simdata.cpp:245-254)."""
+    terr = np.zeros((8, 8), np.float32)
+    synth.write_grid(str(tmp_path / "t.bin"), terr)
+    y = tmp_path / "d.yml"
+    y.write_text(f"name: {tmp_path}/d\nterrain: [{tmp_path}/t.bin, 0]\nW: 8\nH: 8\ndx: 2\ndt: 0.1\n"
+                 f"duration: 60*2\n")
+    cfg = config_json(str(y))
+    assert cfg["variable_dt"] is True and cfg["kSt"] == 30.0 and cfg["no_data"] == -9999.0
+    assert cfg["target_duration"] == 120.0  # solveSimpleMathExpression: products
+
+
+def test_gauge_series_with_dates(tmp_path):
+    """A real-gauge style record: %d.%m.%Y %H:%M:%S stamps counted from the first row, CRLF
+    line ends, a header, 15-minute readings over 40 days; the library and the oracle agree."""
+    n = 40 * 96
+    t = np.arange(n) * 900.0
+    q = 50.0 + 40.0 * np.sin(t / 86400.0 * 2 * np.pi) ** 2
+    z = 1.0 + 0.01 * np.sqrt(q)
+    qp, zp = tmp_path / "gauge_q.csv", tmp_path / "gauge_z.csv"
+    synth.write_series(str(qp), t, q, header="date;discharge", dates=True)
+    synth.write_series(str(zp), t, z, header="date;stage", dates=True)
+    for p in (qp, zp):
+        p.write_bytes(p.read_bytes().replace(b"\n", b"\r\n"))
+    terr = np.zeros((16, 16), np.float32)
+    synth.write_grid(str(tmp_path / "t.bin"), terr)
+    y = tmp_path / "g.yml"
+    y.write_text(f"name: {tmp_path}/g\nterrain: [{tmp_path}/t.bin, 0]\nW: 16\nH: 16\ndx: 2\ndt: 0.1\n"
+                 f"duration: 100\nvariable_dt: false\nboundary_conditions:\n"
+                 f"  - side: left\n    type: q\n    q: [{qp}, 0, 1]\n    z: [{zp}, 0, 1]\n    from: 2\n    to: 12\n")
+    cfg = config_json(str(y))
+    b = cfg["boundary_conditions"][0]
+    assert b["series"] and len(b["q_t"]) == n
+    assert np.array_equal(np.float32(b["q_t"]), t.astype(np.float32))
+    assert np.array_equal(np.float32(b["q_v"]), q.astype(np.float32))
+    ot, ov = pyoracle.read_series(str(zp), 0, 1)
+    assert np.array_equal(np.float32(b["z_t"]), np.float32(ot)) and np.array_equal(np.float32(b["z_v"]), np.float32(ov))
+
+
+def test_boundary_program_compiles_for_sm100a(tmp_path):
+    sc = synth.scenario1(str(tmp_path), W=64, H=48, seed=2, duration=600.0, name="p")
+    src = bc_program(sc.yaml_path, 128, compile=True)
+    assert "fip_post" in src and "fip_interp_block" in src and "fip_sum_depths" in src
