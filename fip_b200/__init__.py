@@ -105,6 +105,14 @@ class Simulation:
         _lib.check(_lib.lib().fip_step_timed(self._h, int(n), ctypes.byref(t), ctypes.byref(a), ctypes.byref(b)))
         return t.value, a.value, b.value
 
+    # -- headless colour map ----------------------------------------------------------------
+    def render(self, what: str = "depth", vmax: float = 0.0, png_path: str | None = None) -> np.ndarray:
+        """RGBA8 image (H, W, 4), row 0 = northern edge; optionally also written as a PNG."""
+        img = np.empty((self.H, self.W, 4), np.uint8)
+        _lib.check(_lib.lib().fip_render(self._h, _lib.RENDER[what], float(vmax), img.ctypes.data_as(ctypes.c_void_p),
+                                         os.fspath(png_path).encode() if png_path else None))
+        return img
+
     # -- exact resume ----------------------------------------------------------------------
     def checkpoint(self, path: str) -> None:
         """Writes both ping-pong buffers, hmax and the step state; see restore()."""
@@ -188,6 +196,14 @@ class Ensemble:
         _lib.check(_lib.lib().fip_ensemble_get_field(self._h, int(member), FIELDS[name],
                                                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
+
+    def render(self, member: int, what: str = "hmax", vmax: float = 0.0, png_path: str | None = None) -> np.ndarray:
+        H, W = self.shapes[member]
+        img = np.empty((H, W, 4), np.uint8)
+        _lib.check(_lib.lib().fip_ensemble_render(self._h, int(member), _lib.RENDER[what], float(vmax),
+                                                  img.ctypes.data_as(ctypes.c_void_p),
+                                                  os.fspath(png_path).encode() if png_path else None))
+        return img
 
     def time(self, member: int):
         d, dt, it = ctypes.c_double(), ctypes.c_float(), ctypes.c_int()

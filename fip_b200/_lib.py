@@ -21,6 +21,8 @@ FIP_ERR_NONFINITE = -5
 FIP_ERR_DEVICE_TIMEOUT = -6
 FIP_ERR_ARG = -7
 
+RENDER = {"depth": 0, "velocity": 1, "hmax": 2}
+
 FIELDS = {"h": 0, "qx": 1, "qy": 2, "hmax": 3, "h_prev": 4, "qx_prev": 5, "qy_prev": 6, "terrain": 7, "z": 8}
 
 # every symbol include/fip.h declares
@@ -29,7 +31,7 @@ EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_ru
            "fip_last_error", "fip_validate", "fip_config_json", "fip_bc_program",
            "fip_ensemble_init", "fip_ensemble_step", "fip_ensemble_run", "fip_ensemble_autotune", "fip_ensemble_set_shape",
            "fip_ensemble_step_timed", "fip_ensemble_get_field", "fip_ensemble_time", "fip_ensemble_info",
-           "fip_ensemble_destroy", "fip_checkpoint", "fip_restore")
+           "fip_ensemble_destroy", "fip_checkpoint", "fip_restore", "fip_render", "fip_ensemble_render")
 
 
 class FipOptions(ctypes.Structure):
@@ -105,6 +107,10 @@ def lib():
         L.fip_ensemble_info.argtypes = [vp, ctypes.POINTER(EnsembleInfo)]
         L.fip_ensemble_destroy.argtypes = [vp]
         L.fip_ensemble_destroy.restype = None
+        L.fip_render.argtypes = [vp, ip, ctypes.c_float, vp, ctypes.c_char_p]
+        L.fip_render.restype = ctypes.c_int
+        L.fip_ensemble_render.argtypes = [vp, ip, ip, ctypes.c_float, vp, ctypes.c_char_p]
+        L.fip_ensemble_render.restype = ctypes.c_int
         L.fip_checkpoint.argtypes = [vp, ctypes.c_char_p]
         L.fip_restore.argtypes = [vp, ctypes.c_char_p]
         L.fip_checkpoint.restype = ctypes.c_int

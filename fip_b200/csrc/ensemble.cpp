@@ -34,10 +34,14 @@
 #include "drv.h"
 #include "fip.h"
 #include "fip_ctl.h"
+#include "render.h"
 #include "rmg_stencil.h"
 
 namespace fip {
 void set_last_error(const std::string& msg);
+int render_region(int device, cudaStream_t stream, const float* h, const float* qx, const float* qy,
+                  const float* sohle, int W, int H, int pitch, float no_value, int what, float vmax,
+                  unsigned char* rgba_or_null, const char* png_path_or_null);
 }
 
 namespace {
@@ -685,6 +689,26 @@ int fip_ensemble_info(fip_ensemble* e, fip_ensemble_info_t* out) {
     }
     out->nonfinite = e->h_ctl->nonfinite;
     return FIP_OK;
+  });
+}
+
+int fip_ensemble_render(fip_ensemble* e, int member, int what, float vmax, unsigned char* rgba_or_null,
+                        const char* png_path_or_null) {
+  if (!e) return efail(FIP_ERR_ARG, "null ensemble");
+  if (member < 0 || member >= e->n) return efail(FIP_ERR_ARG, "fip_ensemble_render: member out of range");
+  return eguard([&] {
+    eck(cudaSetDevice(e->device), "cudaSetDevice");
+    if (what == FIP_RENDER_HMAX) {  // the fold of the member's last step, as fip_ensemble_get_field does
+      std::vector<float> tmp((size_t)e->mem[member].W * e->mem[member].H);
+      const int rc = fip_ensemble_get_field(e, member, FIP_FIELD_HMAX, tmp.data());
+      if (rc) return rc;
+    }
+    const FipEnsMember& M = e->mem[member];
+    const int p = e->parity_of(member);
+    const size_t off = (size_t)M.row_off * e->pitch;
+    const float* src = what == FIP_RENDER_HMAX ? e->st.hmax + off : e->st.h[p] + off;
+    return fip::render_region(e->device, e->stream, src, e->st.qx[p] + off, e->st.qy[p] + off, e->st.sohle + off, M.W,
+                              M.H, e->pitch, M.no_value, what, vmax, rgba_or_null, png_path_or_null);
   });
 }
 

@@ -31,6 +31,7 @@
 #include "drv.h"
 #include "fip.h"
 #include "fip_ctl.h"
+#include "render.h"
 #include "rmg_stencil.h"
 
 namespace {
@@ -494,6 +495,34 @@ int guard(const std::function<int()>& f) {
 
 }  // namespace
 
+namespace fip {
+
+// Renders one field of a grid (pointers at its first row) to rgba_or_null and/or a PNG file.
+int render_region(int device, cudaStream_t stream, const float* h, const float* qx, const float* qy,
+                  const float* sohle, int W, int H, int pitch, float no_value, int what, float vmax,
+                  unsigned char* rgba_or_null, const char* png_path_or_null) {
+  (void)device;
+  if (what < FIP_RENDER_DEPTH || what > FIP_RENDER_HMAX) return fail(FIP_ERR_ARG, "fip_render: unknown field to render");
+  if (!(vmax > 0.f)) vmax = 5.0f;  // the viewer's default scale: 5 m, 5 m/s (src/vis.cpp:264-265)
+  const size_t n = (size_t)W * H * 4;
+  unsigned char* d = nullptr;
+  ck(cudaMallocAsync((void**)&d, n, stream), "fip_render");
+  std::vector<unsigned char> img(n);
+  cudaError_t e = launch_render(h, qx, qy, sohle, W, H, pitch, no_value, what, vmax, d, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(img.data(), d, n, cudaMemcpyDeviceToHost, stream);
+  cudaFreeAsync(d, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  ck(e, "fip_render");
+  if (rgba_or_null) std::memcpy(rgba_or_null, img.data(), n);
+  if (png_path_or_null) {
+    const std::string err = write_png_rgba(png_path_or_null, img.data(), W, H);
+    if (!err.empty()) throw std::invalid_argument("IO:" + err);
+  }
+  return FIP_OK;
+}
+
+}  // namespace fip
+
 extern "C" {
 
 void fip_default_options(fip_options* o) {
@@ -678,6 +707,18 @@ int fip_restore(fip_handle* h, const char* path) {
     h->replan = false;
     ck(cudaStreamSynchronize(h->stream), "restore");
     return FIP_OK;
+  });
+}
+
+int fip_render(fip_handle* h, int what, float vmax, unsigned char* rgba_or_null, const char* png_path_or_null) {
+  if (!h) return fail(FIP_ERR_ARG, "null handle");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    if (what == FIP_RENDER_HMAX) h->flush_hmax_if_due();
+    const int p = h->h_ctl->parity;
+    const float* src = what == FIP_RENDER_HMAX ? h->st.hmax : h->st.h[p];
+    return fip::render_region(h->device, h->stream, src, h->st.qx[p], h->st.qy[p], h->st.sohle, h->st.W, h->st.H,
+                              h->st.pitch, h->st.no_value, what, vmax, rgba_or_null, png_path_or_null);
   });
 }
 

@@ -133,6 +133,17 @@ int fip_checkpoint(fip_handle* h, const char* path);
  * terrain, checked); the run then continues bit for bit as if it had never stopped. */
 int fip_restore(fip_handle* h, const char* path);
 
+/* Headless colour map of the current state, replacing the reference's OpenGL view
+ * (src/vis.cpp, fragment shader src/shaders.h:57-123) with an RGBA8 image seen from straight
+ * above: row 0 is the northern edge (grid row H-1), no-data cells are transparent, water deeper
+ * than 1 cm is coloured with the MATLAB jet map of min(1, value / vmax), dry cells show the
+ * shaded terrain. what: FIP_RENDER_DEPTH, FIP_RENDER_VELOCITY or FIP_RENDER_HMAX; vmax <= 0
+ * uses the viewer's default 5 (m or m/s). Writes W*H*4 bytes to rgba_or_null and/or a PNG file. */
+#define FIP_RENDER_DEPTH 0
+#define FIP_RENDER_VELOCITY 1
+#define FIP_RENDER_HMAX 2
+int fip_render(fip_handle* h, int what, float vmax, unsigned char* rgba_or_null, const char* png_path_or_null);
+
 /* Frees every device and host resource of the handle (the reference leaves this to
  * cudaDeviceReset at exit, src/main.cpp:256). */
 void fip_destroy(fip_handle* h);
@@ -222,6 +233,9 @@ int fip_ensemble_step_timed(fip_ensemble* e, int n_steps, float* total_ms);
 int fip_ensemble_get_field(fip_ensemble* e, int member, int field, float* host);
 int fip_ensemble_time(fip_ensemble* e, int member, double* duration, float* dt, int* iteration);
 int fip_ensemble_info(fip_ensemble* e, fip_ensemble_info_t* out);
+/* fip_render for one member of an ensemble. */
+int fip_ensemble_render(fip_ensemble* e, int member, int what, float vmax, unsigned char* rgba_or_null,
+                        const char* png_path_or_null);
 void fip_ensemble_destroy(fip_ensemble* e);
 
 /* Message of the last failed call on this thread ("" if none). */
