@@ -31,7 +31,8 @@ EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_ru
            "fip_last_error", "fip_validate", "fip_config_json", "fip_bc_program",
            "fip_ensemble_init", "fip_ensemble_step", "fip_ensemble_run", "fip_ensemble_autotune", "fip_ensemble_set_shape",
            "fip_ensemble_step_timed", "fip_ensemble_get_field", "fip_ensemble_time", "fip_ensemble_info",
-           "fip_ensemble_destroy", "fip_checkpoint", "fip_restore", "fip_render", "fip_ensemble_render")
+           "fip_ensemble_destroy", "fip_checkpoint", "fip_restore", "fip_render", "fip_ensemble_render",
+           "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad")
 
 
 class FipOptions(ctypes.Structure):
