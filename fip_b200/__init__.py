@@ -205,6 +205,12 @@ class Ensemble:
                                                   os.fspath(png_path).encode() if png_path else None))
         return img
 
+    def gather(self, name: str, out) -> None:
+        """Every member's field, one grid after the other, into device memory `out` (a CUDA
+        tensor or device pointer of sum(W * H) floats)."""
+        ptr = out if isinstance(out, int) else out.data_ptr()
+        _lib.check(_lib.lib().fip_ensemble_gather(self._h, FIELDS[name], ctypes.c_void_p(ptr)))
+
     def time(self, member: int):
         d, dt, it = ctypes.c_double(), ctypes.c_float(), ctypes.c_int()
         _lib.check(_lib.lib().fip_ensemble_time(self._h, int(member), ctypes.byref(d), ctypes.byref(dt),

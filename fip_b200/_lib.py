@@ -32,7 +32,9 @@ EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_ru
            "fip_ensemble_init", "fip_ensemble_step", "fip_ensemble_run", "fip_ensemble_autotune", "fip_ensemble_set_shape",
            "fip_ensemble_step_timed", "fip_ensemble_get_field", "fip_ensemble_time", "fip_ensemble_info",
            "fip_ensemble_destroy", "fip_checkpoint", "fip_restore", "fip_render", "fip_ensemble_render",
-           "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad")
+           "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad", "fip_ensemble_gather", "fip_sg_pack_input", "fip_sg_target",
+           "fip_sg_loss", "fip_sg_bias_grad", "fip_sg_adamw", "fip_sg_cast_weights", "fip_sg_apply",
+           "fip_sg_edge_flux", "fip_sg_pin")
 
 
 class FipOptions(ctypes.Structure):
@@ -112,6 +114,24 @@ def lib():
         L.fip_render.restype = ctypes.c_int
         L.fip_ensemble_render.argtypes = [vp, ip, ip, ctypes.c_float, vp, ctypes.c_char_p]
         L.fip_ensemble_render.restype = ctypes.c_int
+        L.fip_ensemble_gather.argtypes = [vp, ip, vp]
+        f32, ll = ctypes.c_float, ctypes.c_longlong
+        L.fip_sg_conv3x3.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, vp, vp]
+        L.fip_sg_conv3x3_wgrad.argtypes = [vp, vp, vp, ip, ip, ip, vp, vp]
+        L.fip_sg_pack_input.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, f32, vp, vp]
+        L.fip_sg_target.argtypes = [vp, vp, vp, vp, vp, vp, vp, ll, f32, vp, vp]
+        L.fip_sg_loss.argtypes = [vp, vp, ip, ip, ip, vp, vp, vp]
+        L.fip_sg_bias_grad.argtypes = [vp, ll, vp, vp]
+        L.fip_sg_adamw.argtypes = [vp, vp, vp, vp, ll, f32, f32, f32, f32, f32, ip, vp]
+        L.fip_sg_cast_weights.argtypes = [vp, ip, vp, vp, vp]
+        L.fip_sg_apply.argtypes = [vp, ip, ip, ip, vp, f32, vp, vp, vp, vp, vp]
+        L.fip_sg_edge_flux.argtypes = [vp, vp, ip, ip, ip, vp, vp]
+        L.fip_sg_pin.argtypes = [vp, vp, vp, vp, ll, vp, vp, vp, vp]
+        L.fip_sg_pin.restype = ctypes.c_int
+        for name in ("fip_ensemble_gather", "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad", "fip_sg_pack_input",
+                     "fip_sg_target", "fip_sg_loss", "fip_sg_bias_grad", "fip_sg_adamw", "fip_sg_cast_weights",
+                     "fip_sg_apply", "fip_sg_edge_flux"):
+            getattr(L, name).restype = ctypes.c_int
         L.fip_checkpoint.argtypes = [vp, ctypes.c_char_p]
         L.fip_restore.argtypes = [vp, ctypes.c_char_p]
         L.fip_checkpoint.restype = ctypes.c_int

@@ -654,6 +654,34 @@ int fip_ensemble_get_field(fip_ensemble* e, int member, int field, float* host) 
   });
 }
 
+int fip_ensemble_gather(fip_ensemble* e, int field, float* dev_out) {
+  if (!e || !dev_out) return efail(FIP_ERR_ARG, "null argument");
+  return eguard([&] {
+    eck(cudaSetDevice(e->device), "cudaSetDevice");
+    size_t off_out = 0;
+    for (int m = 0; m < e->n; ++m) {
+      const FipEnsMember& M = e->mem[m];
+      const int p = e->parity_of(m);
+      const float* src = nullptr;
+      switch (field) {
+        case FIP_FIELD_H: src = e->st.h[p]; break;
+        case FIP_FIELD_QX: src = e->st.qx[p]; break;
+        case FIP_FIELD_QY: src = e->st.qy[p]; break;
+        case FIP_FIELD_HMAX: src = e->st.hmax; break;
+        case FIP_FIELD_TERRAIN: src = e->st.sohle; break;
+        default: throw std::invalid_argument("fip_ensemble_gather: unsupported field");
+      }
+      const size_t rb = (size_t)M.W * sizeof(float);
+      eck(cudaMemcpy2DAsync(dev_out + off_out, rb, src + (size_t)M.row_off * e->pitch, (size_t)e->pitch * sizeof(float),
+                            rb, M.H, cudaMemcpyDeviceToDevice, e->stream),
+          "fip_ensemble_gather");
+      off_out += (size_t)M.W * M.H;
+    }
+    eck(cudaStreamSynchronize(e->stream), "fip_ensemble_gather");
+    return FIP_OK;
+  });
+}
+
 int fip_ensemble_time(fip_ensemble* e, int member, double* duration, float* dt, int* iteration) {
   if (!e) return efail(FIP_ERR_ARG, "null ensemble");
   if (member < 0 || member >= e->n) return efail(FIP_ERR_ARG, "fip_ensemble_time: member out of range");

@@ -72,4 +72,65 @@ int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H,
                  "fip_sg_conv3x3_wgrad");
 }
 
+#define SG_S static_cast<cudaStream_t>(stream)
+
+int fip_sg_pack_input(const float* h, const float* qx, const float* qy, const float* terrain, const float* kst,
+                      const float* zref, int N, int H, int W, float no_value, void* out, void* stream) {
+  if (!h || !qx || !qy || !terrain || !kst || !zref || !out || N <= 0 || H <= 0 || W <= 0)
+    return sg_fail(FIP_ERR_ARG, "fip_sg_pack_input: bad argument");
+  return sg_cuda(fip::sg::pack_input(h, qx, qy, terrain, kst, zref, N, H, W, no_value, static_cast<__nv_bfloat16*>(out),
+                                     SG_S),
+                 "fip_sg_pack_input");
+}
+
+int fip_sg_target(const float* h0, const float* qx0, const float* qy0, const float* h1, const float* qx1,
+                  const float* qy1, const float* terrain, long long total, float no_value, float* tgt, void* stream) {
+  if (!h0 || !qx0 || !qy0 || !h1 || !qx1 || !qy1 || !terrain || !tgt || total <= 0)
+    return sg_fail(FIP_ERR_ARG, "fip_sg_target: bad argument");
+  return sg_cuda(fip::sg::make_target(h0, qx0, qy0, h1, qx1, qy1, terrain, (size_t)total, no_value, tgt, SG_S),
+                 "fip_sg_target");
+}
+
+int fip_sg_loss(const float* pred, const float* tgt, int N, int H, int W, void* grad, double* loss, void* stream) {
+  if (!pred || !tgt || !grad || !loss || N <= 0 || H <= 0 || W <= 0) return sg_fail(FIP_ERR_ARG, "fip_sg_loss: bad argument");
+  return sg_cuda(fip::sg::loss_and_grad(pred, tgt, N, H, W, static_cast<__nv_bfloat16*>(grad), loss, SG_S), "fip_sg_loss");
+}
+
+int fip_sg_bias_grad(const void* g, long long n_pix, float* db, void* stream) {
+  if (!g || !db || n_pix <= 0) return sg_fail(FIP_ERR_ARG, "fip_sg_bias_grad: bad argument");
+  return sg_cuda(fip::sg::bias_grad(static_cast<const __nv_bfloat16*>(g), (size_t)n_pix, db, SG_S), "fip_sg_bias_grad");
+}
+
+int fip_sg_adamw(float* p, const float* g, float* m, float* v, long long n, float lr, float beta1, float beta2,
+                 float eps, float weight_decay, int step, void* stream) {
+  if (!p || !g || !m || !v || n <= 0 || step < 1) return sg_fail(FIP_ERR_ARG, "fip_sg_adamw: bad argument");
+  return sg_cuda(fip::sg::adamw(p, g, m, v, (size_t)n, lr, beta1, beta2, eps, weight_decay, step, SG_S), "fip_sg_adamw");
+}
+
+int fip_sg_cast_weights(const float* p, int n_layers, void* wf, void* wd, void* stream) {
+  if (!p || !wf || !wd || n_layers <= 0) return sg_fail(FIP_ERR_ARG, "fip_sg_cast_weights: bad argument");
+  return sg_cuda(fip::sg::cast_weights(p, n_layers, static_cast<__nv_bfloat16*>(wf), static_cast<__nv_bfloat16*>(wd),
+                                       SG_S),
+                 "fip_sg_cast_weights");
+}
+
+int fip_sg_apply(const float* pred, int N, int H, int W, const float* terrain, float no_value, float* h, float* qx,
+                 float* qy, double* dvol, void* stream) {
+  if (!pred || !terrain || !h || !qx || !qy || !dvol || N <= 0 || (long long)H * W < 256)
+    return sg_fail(FIP_ERR_ARG, "fip_sg_apply: bad argument (images of at least 256 cells)");
+  return sg_cuda(fip::sg::apply_update(pred, N, H, W, terrain, no_value, h, qx, qy, dvol, SG_S), "fip_sg_apply");
+}
+
+int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, void* stream) {
+  if (!qx || !qy || !flux || N <= 0 || H < 3 || W < 3) return sg_fail(FIP_ERR_ARG, "fip_sg_edge_flux: bad argument");
+  return sg_cuda(fip::sg::edge_flux(qx, qy, N, H, W, flux, SG_S), "fip_sg_edge_flux");
+}
+
+int fip_sg_pin(const unsigned char* mask, const float* h_val, const float* qx_val, const float* qy_val, long long total,
+               float* h, float* qx, float* qy, void* stream) {
+  if (!mask || !h_val || !qx_val || !qy_val || !h || !qx || !qy || total <= 0)
+    return sg_fail(FIP_ERR_ARG, "fip_sg_pin: bad argument");
+  return sg_cuda(fip::sg::pin_cells(mask, h_val, qx_val, qy_val, (size_t)total, h, qx, qy, SG_S), "fip_sg_pin");
+}
+
 }  // extern "C"

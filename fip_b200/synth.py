@@ -120,23 +120,23 @@ def terrain0(W: int, H: int, dx: float, seed: int) -> np.ndarray:
 def scenario0(outdir: str, W: int = 1024, H: int = 1024, dx: float = 3.0, dt: float = 0.1,
               duration: float = 1000.0, save_every: float = 100.0, seed: int = 0,
               sampling_interval: int = 0, variable_dt: bool = False, name: str = "scenario0",
-              bc_rows: tuple[int, int] | None = None) -> Scenario:
+              bc_rows: tuple[int, int] | None = None, kst: float = 30.0, level_add: float = 0.0) -> Scenario:
     os.makedirs(outdir, exist_ok=True)
     terr = terrain0(W, H, dx, seed)
     if bc_rows is None:
         bc_rows = (480, 544) if (W, H) == (1024, 1024) else (H // 2 - H // 16, H // 2 + H // 16)
     lo, hi = bc_rows
-    zbc = float(terr[lo:hi + 1, 0].min()) + 2.5
+    zbc = float(terr[lo:hi + 1, 0].min()) + 2.5 + level_add
     tpath = os.path.join(outdir, f"{name}_terrain.bin")
     write_grid(tpath, terr)
     cfg = {
         "#0": f"seed {seed}: terrain0(W={W}, H={H}, dx={dx}); left z level = min terrain of rows "
-              f"{lo}-{hi} + 2.5 m",
+              f"{lo}-{hi} + 2.5 m + {level_add:.6g} m; kSt {kst:.6g}",
         "name": os.path.join(outdir, name),
         "terrain": [tpath, 0],
         "W": W, "H": H, "dx": dx, "dt": dt,
         "duration": duration,
-        "kSt": 30,
+        "kSt": 30 if kst == 30.0 else f"{kst:.9g}",
         "variable_dt": variable_dt,
         "boundary_conditions": [
             {"side": "left", "type": "z", "z": f"{zbc:.9g}", "from": lo, "to": hi},

@@ -231,6 +231,9 @@ int fip_ensemble_set_shape(fip_ensemble* e, int consumer_warps, int tile_rows);
 int fip_ensemble_step_timed(fip_ensemble* e, int n_steps, float* total_ms);
 /* Member field (FIP_FIELD_H .. FIP_FIELD_TERRAIN) into a W x H host buffer. */
 int fip_ensemble_get_field(fip_ensemble* e, int member, int field, float* host);
+/* Member fields (FIP_FIELD_H, _QX, _QY, _HMAX or _TERRAIN) of all members, one W x H grid after
+ * the other, into device memory (sum of the members' W * H floats). */
+int fip_ensemble_gather(fip_ensemble* e, int field, float* dev_out);
 int fip_ensemble_time(fip_ensemble* e, int member, double* duration, float* dt, int* iteration);
 int fip_ensemble_info(fip_ensemble* e, fip_ensemble_info_t* out);
 /* fip_render for one member of an ensemble. */

@@ -30,6 +30,40 @@ int fip_sg_conv3x3(const void* in, const void* w, const float* bias, const void*
 /* dw (f32 [9][64 out][64 in]) = sum over pixels of x[p + tap offset][in] * dy[p][out]. */
 int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H, int W, int* dev_err, void* stream);
 
+/* ---- element-wise kernels; grids are f32 [N][H][W] (row 0 = southern edge) ---- */
+
+/* Network input [N][H+2][W+2][64] bf16: (terrain - zref[n]) * 0.1, kSt * 0.025,
+ * (h + terrain - zref[n]) * 0.1, qx * 0.2, qy * 0.2, (h > 1 cm); zero on no-data cells and in
+ * channels 6..63. */
+int fip_sg_pack_input(const float* h, const float* qx, const float* qy, const float* terrain, const float* kst,
+                      const float* zref, int N, int H, int W, float no_value, void* out, void* stream);
+/* Training target f32 [N][H][W][3]: (h1 - h0) / 0.5, (qx1 - qx0) / 1, (qy1 - qy0) / 1. */
+int fip_sg_target(const float* h0, const float* qx0, const float* qy0, const float* h1, const float* qx1,
+                  const float* qy1, const float* terrain, long long total, float no_value, float* tgt, void* stream);
+/* *loss += sum of squared errors of pred (f32 [N][H+2][W+2][4]) against tgt; grad (bf16
+ * [N][H+2][W+2][64], channels 0..2) = d(mean squared error)/d(pred). grad must be zeroed first. */
+int fip_sg_loss(const float* pred, const float* tgt, int N, int H, int W, void* grad, double* loss, void* stream);
+/* db[c] += sum over pixels of g[p][c] (bf16 [n_pix][64]). */
+int fip_sg_bias_grad(const void* g, long long n_pix, float* db, void* stream);
+/* AdamW step (step >= 1) over n parameters laid out as layers of 9*64*64 weights + 64 biases;
+ * decoupled weight decay on the weights only. */
+int fip_sg_adamw(float* p, const float* g, float* m, float* v, long long n, float lr, float beta1, float beta2,
+                 float eps, float weight_decay, int step, void* stream);
+/* bf16 copies of n_layers layers of f32 parameters: wf [l][9][out][in] for the forward
+ * convolution, wd [l][9][in][out] with reversed taps for the input gradient. */
+int fip_sg_cast_weights(const float* p, int n_layers, void* wf, void* wd, void* stream);
+/* One surrogate call: h = max(0, h + 0.5 * pred0), qx += pred1, qy += pred2 (no-data cells kept);
+ * dvol[n] += change of the depth sum over the inner cells [1, W-2] x [1, H-2] of image n
+ * (H * W >= 256). */
+int fip_sg_apply(const float* pred, int N, int H, int W, const float* terrain, float no_value, float* h, float* qx,
+                 float* qy, double* dvol, void* stream);
+/* flux[n] = net discharge per unit width into the inner cells of image n. */
+int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, void* stream);
+
+/* Cells fixed by boundary conditions: mask bit 0 sets h, bit 1 qx, bit 2 qy to the given values. */
+int fip_sg_pin(const unsigned char* mask, const float* h_val, const float* qx_val, const float* qy_val, long long total,
+               float* h, float* qx, float* qy, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,88 @@
+"""Training kernels of the surrogate: forward pass, loss and every parameter gradient of the
+18-layer network against the FP64 CPU oracle (oracle/surrogate_oracle.py), and a short
+training run that must reduce the loss."""
+import numpy as np
+import pytest
+
+import surrogate_oracle as so
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _bf16_round(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16).float().numpy()
+
+
+def _net(seed):
+    from fip_b200 import surrogate
+
+    p = surrogate.init_params(seed)
+    rng = np.random.default_rng(seed + 1)
+    L = so.LAYER
+    # a non-zero head and biases so that every gradient path carries signal
+    p[17 * L:17 * L + so.TAP] = (rng.standard_normal(so.TAP) * 0.02).astype(np.float32)
+    for l in range(18):
+        p[l * L + so.TAP:(l + 1) * L] = (rng.standard_normal(64) * 0.05).astype(np.float32)
+    for l in range(18):  # the GPU computes with bf16 weights: compare on the same weights
+        p[l * L:l * L + so.TAP] = _bf16_round(p[l * L:l * L + so.TAP])
+    return p
+
+
+def test_gradients_match_fp64_oracle():
+    from fip_b200.surrogate import Surrogate
+
+    N, H, W = 2, 12, 14
+    rng = np.random.default_rng(3)
+    p = _net(5)
+    x = np.zeros((N, H, W, 64), np.float32)
+    x[..., :6] = _bf16_round(rng.standard_normal((N, H, W, 6)) * 0.7)
+    tgt = (rng.standard_normal((N, H, W, 3)) * 0.1).astype(np.float32)
+    net = Surrogate(params=p)
+    b = net._buffers(N, H, W, True)
+    xp = np.pad(x, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    b["x"].copy_(torch.from_numpy(xp).to(torch.bfloat16))
+    pred = net.forward(N, H, W, train=True)
+    dt = torch.from_numpy(tgt).cuda()
+    net.loss_acc.zero_()
+    net.loss(dt, N, H, W)
+    net.backward(N, H, W)
+    net.check_device()
+    ref_loss, ref_g, ref_pred = so.loss_and_grads(p.astype(np.float64), x.astype(np.float64), tgt.astype(np.float64))
+    got_pred = pred.cpu().numpy()[:, 1:-1, 1:-1, :3]
+    assert np.max(np.abs(got_pred - ref_pred[..., :3])) <= 0.02 * np.max(np.abs(ref_pred[..., :3]))
+    got_loss = float(net.loss_acc.item()) / tgt.size
+    assert abs(got_loss - ref_loss) <= 0.02 * ref_loss
+    g = net.g.cpu().numpy().astype(np.float64)
+    for l in range(18):
+        sl = slice(l * so.LAYER, (l + 1) * so.LAYER)
+        num = np.linalg.norm(g[sl] - ref_g[sl])
+        den = np.linalg.norm(ref_g[sl])
+        assert num <= 0.05 * den, (l, num / den)
+
+
+def test_training_reduces_loss():
+    from fip_b200.surrogate import Surrogate
+
+    N, H, W = 4, 32, 40
+    rng = np.random.default_rng(9)
+    x = np.zeros((N, H + 2, W + 2, 64), np.float32)
+    x[:, 1:-1, 1:-1, :6] = rng.standard_normal((N, H, W, 6)) * 0.5
+    # a smooth function of the inputs the network can fit
+    tgt = np.stack([np.tanh(x[:, 1:-1, 1:-1, 0] + x[:, 1:-1, 1:-1, 2]), 0.5 * x[:, 1:-1, 1:-1, 3],
+                    -0.3 * x[:, 1:-1, 1:-1, 4]], -1).astype(np.float32)
+    net = Surrogate(seed=1)
+    b = net._buffers(N, H, W, True)
+    b["x"].copy_(torch.from_numpy(x).to(torch.bfloat16))
+    dt = torch.from_numpy(tgt).cuda()
+    losses = []
+    for it in range(120):
+        net.forward(N, H, W, train=True)
+        net.loss_acc.zero_()
+        net.loss(dt, N, H, W)
+        net.backward(N, H, W)
+        net.update(lr=2e-3)
+        if it % 20 == 0 or it == 119:
+            losses.append(float(net.loss_acc.item()) / tgt.size)
+    net.check_device()
+    assert losses[-1] < 0.2 * losses[0], losses
