@@ -124,7 +124,7 @@ def lib():
         L.fip_sg_bias_grad.argtypes = [vp, ll, vp, vp]
         L.fip_sg_adamw.argtypes = [vp, vp, vp, vp, ll, f32, f32, f32, f32, f32, ip, vp]
         L.fip_sg_cast_weights.argtypes = [vp, ip, vp, vp, vp]
-        L.fip_sg_apply.argtypes = [vp, ip, ip, ip, vp, f32, vp, vp, vp, vp, vp]
+        L.fip_sg_apply.argtypes = [vp, ip, ip, ip, vp, f32, vp, vp, vp, vp, vp, vp]
         L.fip_sg_edge_flux.argtypes = [vp, vp, ip, ip, ip, vp, vp]
         L.fip_sg_pin.argtypes = [vp, vp, vp, vp, ll, vp, vp, vp, vp]
         L.fip_sg_pin.restype = ctypes.c_int

@@ -115,10 +115,10 @@ int fip_sg_cast_weights(const float* p, int n_layers, void* wf, void* wd, void* 
 }
 
 int fip_sg_apply(const float* pred, int N, int H, int W, const float* terrain, float no_value, float* h, float* qx,
-                 float* qy, double* dvol, void* stream) {
+                 float* qy, double* dvol, float* hmax, void* stream) {
   if (!pred || !terrain || !h || !qx || !qy || !dvol || N <= 0 || (long long)H * W < 256)
     return sg_fail(FIP_ERR_ARG, "fip_sg_apply: bad argument (images of at least 256 cells)");
-  return sg_cuda(fip::sg::apply_update(pred, N, H, W, terrain, no_value, h, qx, qy, dvol, SG_S), "fip_sg_apply");
+  return sg_cuda(fip::sg::apply_update(pred, N, H, W, terrain, no_value, h, qx, qy, dvol, hmax, SG_S), "fip_sg_apply");
 }
 
 int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, void* stream) {

@@ -35,7 +35,9 @@ constexpr int C = 64;                   // channels of every activation tensor
 constexpr int BM = 128;                 // pixels per forward tile (MMA M)
 constexpr int kTapBytes = C * C * 2;    // 8 KB: one tap of the weights, 64 x 64 bf16
 constexpr int kWBytes = 9 * kTapBytes;  // 72 KB
-constexpr int kATileBytes = BM * C * 2; // 16 KB
+constexpr int kSlabRows = 136;         // a tile's 128 rows plus the 2 rows the dx shifts reach, rounded to 8
+constexpr int kSlabBytes = kSlabRows * C * 2;  // 17 KB of one dy slab
+constexpr int kSlabStride = 18 * 1024;  // slabs start on 1024-byte boundaries (swizzle pattern)
 constexpr int kStages = 6;
 constexpr int kThreads = 192;           // warp 0: TMA, warp 1: MMA + TMEM owner, warps 2-5: epilogue
 constexpr unsigned long long kWaitNs = 2000000000ull;
@@ -119,6 +121,8 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 // K-major: rows of 128 B along K, 8-row groups 1024 B apart (SBO), LBO unused (1).
 // MN-major: rows of 128 B hold 64 M/N elements for one K index, 8-K-row groups 1024 B apart
 // (SBO), the next 64 M/N elements `lbo_bytes` further (LBO).
+// The swizzle is applied to absolute shared-memory addresses (as TMA writes them), so a matrix
+// may start at any row or 16-byte column of a 1024-byte-aligned tile (base offset 0).
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
   return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (2ull << 61);
@@ -166,7 +170,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* s_w = smem;                    // 9 taps x 8 KB
-  unsigned char* s_a = smem + kWBytes;          // kStages x 16 KB
+  unsigned char* s_a = smem + kWBytes;          // kStages x 18 KB: one 136-row slab per dy
   __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], w_bar, acc_full[2], acc_empty[2], done_bar;
   __shared__ uint32_t s_tmem;
   __shared__ float s_bias[C];
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ok = true;
       for (int tile = blockIdx.x; ok && tile < a.n_tiles; tile += gridDim.x) {
         const int p0 = tile * BM;
-        for (int t = 0; t < 9; ++t, ++it) {
+        for (int r = 0; r < 3; ++r, ++it) {  // rows p0 + dy * Wp - 1 .. + 134 serve the taps (dy, -1..1)
           const uint32_t st = it % kStages, ph = (it / kStages) & 1u;
           if (!mbar_wait(&empty_bar[st], ph ^ 1u, &s_abort)) {
             record(a.err, 1);
@@ -216,9 +220,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             ok = false;
             break;
           }
-          const int dy = t / 3 - 1, dx = t % 3 - 1;
-          mbar_expect_tx(&full_bar[st], kATileBytes);
-          tma_2d(s_a + st * kATileBytes, &tm_act, 0, p0 + dy * Wp + dx, &full_bar[st]);
+          const int dy = r - 1;
+          mbar_expect_tx(&full_bar[st], kSlabBytes);
+          tma_2d(s_a + st * kSlabStride, &tm_act, 0, p0 + dy * Wp - 1, &full_bar[st]);
         }
       }
     }
@@ -240,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         tc_fence_after();
         const uint32_t d = tmem + acc * C;
-        for (int t = 0; t < 9; ++t, ++it) {
+        for (int r = 0; r < 3; ++r, ++it) {
           const uint32_t st = it % kStages, ph = (it / kStages) & 1u;
           if (!mbar_wait(&full_bar[st], ph, &s_abort)) {
             record(a.err, 4);
@@ -249,10 +253,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           tc_fence_after();
-          const uint32_t sa = smem_u32(s_a + st * kATileBytes), sb = smem_u32(s_w + t * kTapBytes);
+          const uint32_t slab = smem_u32(s_a + st * kSlabStride);
 #pragma unroll
-          for (int k = 0; k < 4; ++k)
-            tc_mma(d, sdesc(sa + 32 * k, 16, 1024), sdesc(sb + 32 * k, 16, 1024), idesc, (t | k) ? 1u : 0u);
+          for (int c = 0; c < 3; ++c) {  // tap (dy, dx = c - 1): the slab from row c on
+            const uint32_t sa = slab + 128 * c, sb = smem_u32(s_w + (3 * r + c) * kTapBytes);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+              tc_mma(d, sdesc(sa + 32 * k, 16, 1024), sdesc(sb + 32 * k, 16, 1024), idesc, (r | c | k) ? 1u : 0u);
+          }
           tc_commit(&empty_bar[st]);
         }
         if (!ok) break;
@@ -519,7 +527,7 @@ cudaError_t conv3x3(const ConvShape& s, const __nv_bfloat16* in, const __nv_bflo
   if (!drv::load(&derr)) return cudaErrorInitializationError;
   const int n_pix = s.N * (s.H + 2) * (s.W + 2);
   CUtensorMap tm_a, tm_w;
-  if (encode_act_map(&tm_a, in, n_pix, BM) || encode_act_map(&tm_w, w, 9 * C, C)) return cudaErrorInvalidValue;
+  if (encode_act_map(&tm_a, in, n_pix, kSlabRows) || encode_act_map(&tm_w, w, 9 * C, C)) return cudaErrorInvalidValue;
   FwdArgs a;
   a.bias = bias;
   a.res = res;
@@ -530,7 +538,7 @@ cudaError_t conv3x3(const ConvShape& s, const __nv_bfloat16* in, const __nv_bflo
   a.Wp = s.W + 2;
   a.n_tiles = (n_pix + BM - 1) / BM;
   a.err = err;
-  const int smem = kWBytes + kStages * kATileBytes + 1024;
+  const int smem = kWBytes + kStages * kSlabStride + 1024;
   const int grid = std::min(conv_grid(), a.n_tiles);
 #define FIP_SG_LAUNCH(E)                                                                                  \
   case E: {                                                                                                \

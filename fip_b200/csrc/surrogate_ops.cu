@@ -139,10 +139,11 @@ __global__ void cast_weights_kernel(const float* __restrict__ p, int n_layers, _
 }
 
 // state update of one surrogate call: h += dz (clamped at 0), qx += dqx, qy += dqy; no-data
-// cells keep their values. dvol[n] += volume change (depth sum) of image n's inner cells.
+// cells keep their values. dvol[n] += volume change (depth sum) of image n's inner cells;
+// hmax (optional) = max(hmax, new depth).
 __global__ void apply_kernel(const float* __restrict__ pred, int N, int H, int W, const float* __restrict__ terr,
                              float no_value, float* __restrict__ h, float* __restrict__ qx, float* __restrict__ qy,
-                             double* __restrict__ dvol) {
+                             double* __restrict__ dvol, float* __restrict__ hmax) {
   __shared__ double red[2][256];
   __shared__ int s_n0;
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,11 +159,12 @@ __global__ void apply_kernel(const float* __restrict__ pred, int N, int H, int W
       const float h0 = h[i];
       const float h1 = fmaxf(0.f, h0 + pred[p * 4 + 0] * kOutZ);
       h[i] = h1;
+      if (hmax) hmax[i] = fmaxf(hmax[i], h1);
       qx[i] += pred[p * 4 + 1] * kOutQ;
       qy[i] += pred[p * 4 + 2] * kOutQ;
-      // volume of the cells the continuity equation updates (the edge cells belong to the
-      // boundary conditions): its change must match the discharge through the inner faces
-      if (x >= 1 && x <= W - 2 && y >= 1 && y <= H - 2) dv = (double)h1 - (double)h0;
+      // volume of the cells only the continuity equation updates (a z condition on the left
+      // edge also sets column 1): its change must match the discharge through the faces around
+      if (x >= 2 && x <= W - 2 && y >= 1 && y <= H - 2) dv = (double)h1 - (double)h0;
     }
   }
   if (threadIdx.x == 0) s_n0 = (int)(((size_t)blockIdx.x * blockDim.x) / img);
@@ -184,18 +186,20 @@ __global__ void apply_kernel(const float* __restrict__ pred, int N, int H, int W
   }
 }
 
-// Net discharge into the inner cells [1, W-2] x [1, H-2] per image (qx sits on east faces,
-// qy on north faces): + qx[y][0] - qx[y][W-2] over the rows, + qy[0][x] - qy[H-2][x] over the
-// columns (a sum of discharges per unit width; times dx gives m3/s).
+// Net discharge into the inner cells [2, W-2] x [1, H-2] per image (qx sits on east faces,
+// qy on north faces): + qx[y][1] - qx[y][W-2] over rows 1..H-2, + qy[0][x] - qy[H-2][x] over
+// columns 2..W-2 (a sum of discharges per unit width; times dx gives m3/s).
 __global__ void edge_flux_kernel(const float* __restrict__ qx, const float* __restrict__ qy, int N, int H, int W,
                                  double* __restrict__ flux) {
   const int n = blockIdx.y;
   double acc = 0.0;
-  for (int k = threadIdx.x; k < H + W; k += blockDim.x) {
-    const size_t base = (size_t)n * H * W;
-    if (k < H) acc += (double)qx[base + (size_t)k * W + 0] - (double)qx[base + (size_t)k * W + (W - 2)];
-    else {
-      const int x = k - H;
+  const size_t base = (size_t)n * H * W;
+  for (int k = threadIdx.x; k < (H - 2) + (W - 3); k += blockDim.x) {
+    if (k < H - 2) {
+      const size_t row = base + (size_t)(k + 1) * W;
+      acc += (double)qx[row + 1] - (double)qx[row + (W - 2)];
+    } else {
+      const int x = 2 + (k - (H - 2));
       acc += (double)qy[base + x] - (double)qy[base + (size_t)(H - 2) * W + x];
     }
   }
@@ -268,9 +272,9 @@ cudaError_t cast_weights(const float* p, int n_layers, __nv_bfloat16* wf, __nv_b
 }
 
 cudaError_t apply_update(const float* pred, int N, int H, int W, const float* terr, float no_value, float* h, float* qx,
-                         float* qy, double* dvol, cudaStream_t s) {
+                         float* qy, double* dvol, float* hmax, cudaStream_t s) {
   const size_t total = (size_t)N * H * W;
-  apply_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(pred, N, H, W, terr, no_value, h, qx, qy, dvol);
+  apply_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(pred, N, H, W, terr, no_value, h, qx, qy, dvol, hmax);
   return cudaGetLastError();
 }
 

@@ -184,17 +184,18 @@ class Surrogate:
         self.cast()
 
     # ---- one surrogate call ------------------------------------------------------------------
-    def advance(self, state, pins=None):
+    def advance(self, state, pins=None, hmax=None):
         """state: dict of device tensors h, qx, qy, terrain, kst [N][H][W], zref [N], no_value;
-        h/qx/qy advance by 60 s in place. Returns the per-image depth-sum change of the inner
-        cells (device double [N])."""
+        h/qx/qy advance by 60 s in place (hmax, if given, folds the new depths). Returns the
+        per-image depth-sum change of the inner cells (device double [N])."""
         h, qx, qy = state["h"], state["qx"], state["qy"]
         N, H, W = h.shape
         self.pack(h, qx, qy, state["terrain"], state["kst"], state["zref"], state["no_value"], N, H, W)
         pred = self.forward(N, H, W)
         dvol = self.torch.zeros(N, dtype=self.torch.float64, device=self.dev)
         _lib.check(self.L.fip_sg_apply(_ptr(pred), N, H, W, _ptr(state["terrain"]), float(state["no_value"]), _ptr(h),
-                                       _ptr(qx), _ptr(qy), _ptr(dvol), _stream()))
+                                       _ptr(qx), _ptr(qy), _ptr(dvol), _ptr(hmax) if hmax is not None else None,
+                                       _stream()))
         if pins is not None:
             _lib.check(self.L.fip_sg_pin(_ptr(pins["mask"]), _ptr(pins["h"]), _ptr(pins["qx"]), _ptr(pins["qy"]),
                                          h.numel(), _ptr(h), _ptr(qx), _ptr(qy), _stream()))
@@ -210,3 +211,40 @@ class Surrogate:
         n = s0["h"].numel()
         _lib.check(self.L.fip_sg_target(_ptr(s0["h"]), _ptr(s0["qx"]), _ptr(s0["qy"]), _ptr(s1["h"]), _ptr(s1["qx"]),
                                         _ptr(s1["qy"]), _ptr(terrain), n, float(no_value), _ptr(out), _stream()))
+
+
+def bench_convs(N: int = 32, H: int = 512, W: int = 512, iters: int = 20, device: int = 0) -> dict:
+    """Device time of one 64 -> 64 3x3 convolution (forward with the bias + ReLU epilogue, input
+    gradient, weight gradient) on an N x H x W batch, CUDA events on the launching stream,
+    after warm-up. FLOPs are the algorithmic 2 * 9 * 64 * 64 per interior pixel."""
+    torch = _torch()
+    net = Surrogate(device=device)
+    L, st, err = net.L, _stream(), _ptr(net.err)
+    b = net._buffers(N, H, W, True)
+    x, y = b["a"][0], b["a"][1]
+    gen = torch.Generator(device=net.dev)
+    gen.manual_seed(0)
+    x.copy_((torch.rand(x.shape, device=net.dev, generator=gen) - 0.5).to(torch.bfloat16))
+    dw = torch.zeros(TAP, dtype=torch.float32, device=net.dev)
+    flop = 2.0 * 9 * C * C * N * H * W
+    res = {}
+    runs = {
+        "forward": lambda: L.fip_sg_conv3x3(_ptr(x), _ptr(net.wf, TAP), _ptr(net.p, LAYER + TAP), None, None, _ptr(y),
+                                            N, H, W, EPI_BIAS_RELU, err, st),
+        "dgrad": lambda: L.fip_sg_conv3x3(_ptr(x), _ptr(net.wd, TAP), None, None, _ptr(x), _ptr(y), N, H, W, EPI_MASK,
+                                          err, st),
+        "wgrad": lambda: L.fip_sg_conv3x3_wgrad(_ptr(x), _ptr(y), _ptr(dw), N, H, W, err, st),
+    }
+    for name, fn in runs.items():
+        for _ in range(3):
+            _lib.check(fn())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(iters):
+            _lib.check(fn())
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / iters
+        res[name] = {"ms": ms, "tflops": flop / (ms * 1e-3) / 1e12}
+    net.check_device()
+    return res

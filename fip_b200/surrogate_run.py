@@ -1,0 +1,300 @@
+"""Training and use of the learned surrogate on trajectories the solver generates.
+
+Workloads:
+  * training data: the plain-solver scenario generator (synth.scenario0: sloping terrain with
+    Gaussian bumps and a channel, left z inflow, right open, top/bottom closed, fixed dt 0.1 s)
+    with fresh seeds, kSt ~ U[20, 45] and the inflow level raised by U[1, 4] m; every member is
+    run by the batched ensemble solver and snapshotted every 60 simulated seconds;
+  * training: pairs (state at t, state at t + 60 s) of those trajectories, AdamW, MSE on the
+    scaled change of depth and discharges;
+  * evaluation: held-out trajectories; one-call (60 s) error against persistence (the method
+    without the network: the state does not change) and closed-loop rollouts;
+  * screening: an ensemble rolled out by the surrogate to max-depth maps; the most flooded
+    fraction and every member whose mass-balance residual trips the fallback are re-run by the
+    batched solver; the result is judged against the batched solver on every member (max-depth
+    RMSE, flooded-extent IoU at 5 cm, wall time).
+
+    python -m fip_b200.surrogate_run [--members 32 --size 512 --hours 1 --steps 400 ...]
+
+prints one JSON object with the measurements.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import tempfile
+import time
+
+import numpy as np
+
+from . import Ensemble, synth
+from .surrogate import Surrogate
+
+CALL_S = 60.0
+DT = 0.1
+STEPS_PER_CALL = int(round(CALL_S / DT))
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def config3_members(outdir: str, n: int, size: int, seed: int, duration: float):
+    """Scenario generator of the surrogate workloads (see module docstring)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        kst = float(rng.uniform(20.0, 45.0))
+        lvl = float(rng.uniform(1.0, 4.0))
+        out.append(synth.scenario0(outdir, W=size, H=size, duration=duration, save_every=0, dt=DT,
+                                   seed=seed * 100003 + i, name=f"s{seed}_{i}", kst=kst, level_add=lvl))
+    return out
+
+
+class Batch:
+    """Static inputs of a set of equally sized scenarios on the GPU."""
+
+    def __init__(self, scenarios, device=0):
+        torch = _torch()
+        self.n = len(scenarios)
+        self.H, self.W = scenarios[0].H, scenarios[0].W
+        dev = torch.device("cuda", device)
+        terr = np.stack([s.terrain for s in scenarios]).astype(np.float32)
+        self.terrain = torch.from_numpy(terr).to(dev)
+        kst = np.stack([np.full((self.H, self.W), float(s.info.get("kst", 30.0)), np.float32) for s in scenarios])
+        self.kst = torch.from_numpy(kst).to(dev)
+        self.zref = torch.from_numpy(terr.reshape(self.n, -1).mean(1).astype(np.float32)).to(dev)
+        # left z condition: h fixed at both boundary columns, qx = 0 on the boundary face
+        mask = np.zeros((self.n, self.H, self.W), np.uint8)
+        hv = np.zeros((self.n, self.H, self.W), np.float32)
+        for k, s in enumerate(scenarios):
+            lo, hi = s.info["bc_rows"]
+            for c in (0, 1):
+                hv[k, lo:hi + 1, c] = np.maximum(0.0, np.float32(s.info["zbc"]) - s.terrain[lo:hi + 1, c])
+                mask[k, lo:hi + 1, c] |= 1
+            mask[k, lo:hi + 1, 0] |= 2
+        self.pins = {"mask": torch.from_numpy(mask).to(dev), "h": torch.from_numpy(hv).to(dev),
+                     "qx": torch.zeros_like(self.terrain), "qy": torch.zeros_like(self.terrain)}
+        self.no_value = -9999.0
+        self.cells = self.n * self.H * self.W
+
+    def state(self, h, qx, qy):
+        return {"h": h, "qx": qx, "qy": qy, "terrain": self.terrain, "kst": self.kst, "zref": self.zref,
+                "no_value": self.no_value}
+
+
+def solver_trajectories(scenarios, n_calls: int, device=0):
+    """Snapshots [n_calls + 1][members][H][W] of h, qx, qy every 60 s (batched solver) and the
+    solver's max-depth maps at the end."""
+    torch = _torch()
+    paths = [s.yaml_path for s in scenarios]
+    B, H, W = len(scenarios), scenarios[0].H, scenarios[0].W
+    snaps = {k: torch.empty((n_calls + 1, B, H, W), dtype=torch.float32, device=torch.device("cuda", device))
+             for k in ("h", "qx", "qy")}
+    t0 = time.perf_counter()
+    with Ensemble(paths, device=device) as e:
+        for k in ("h", "qx", "qy"):
+            e.gather(k, snaps[k][0])
+        for c in range(n_calls):
+            e.step(STEPS_PER_CALL)
+            for k in ("h", "qx", "qy"):
+                e.gather(k, snaps[k][c + 1])
+        hmax = torch.empty((B, H, W), dtype=torch.float32, device=snaps["h"].device)
+        e.gather("hmax", hmax)
+    torch.cuda.synchronize()
+    return snaps, hmax, time.perf_counter() - t0
+
+
+def train(net: Surrogate, batch: Batch, snaps, steps: int, bs: int = 32, lr: float = 1e-3, seed: int = 0,
+          log_every: int = 50):
+    torch = _torch()
+    T = snaps["h"].shape[0] - 1
+    B, H, W = batch.n, batch.H, batch.W
+    dev = snaps["h"].device
+    rng = np.random.default_rng(seed)
+    tgt = torch.empty((bs, H, W, 3), dtype=torch.float32, device=dev)
+    cur = {k: torch.empty((bs, H, W), dtype=torch.float32, device=dev) for k in ("h", "qx", "qy")}
+    nxt = {k: torch.empty((bs, H, W), dtype=torch.float32, device=dev) for k in ("h", "qx", "qy")}
+    terr = torch.empty((bs, H, W), dtype=torch.float32, device=dev)
+    kst = torch.empty_like(terr)
+    zref = torch.empty(bs, dtype=torch.float32, device=dev)
+    log = []
+    t0 = time.perf_counter()
+    for it in range(steps):
+        ti = torch.from_numpy(rng.integers(0, T, bs)).to(dev)
+        mi = torch.from_numpy(rng.integers(0, B, bs)).to(dev)
+        for k in ("h", "qx", "qy"):
+            cur[k].copy_(snaps[k][ti, mi])
+            nxt[k].copy_(snaps[k][ti + 1, mi])
+        terr.copy_(batch.terrain[mi])
+        kst.copy_(batch.kst[mi])
+        zref.copy_(batch.zref[mi])
+        net.target(cur, nxt, terr, batch.no_value, tgt)
+        net.pack(cur["h"], cur["qx"], cur["qy"], terr, kst, zref, batch.no_value, bs, H, W, train=True)
+        net.forward(bs, H, W, train=True)
+        net.loss_acc.zero_()
+        net.loss(tgt, bs, H, W)
+        net.backward(bs, H, W)
+        a = lr * 0.5 * (1 + np.cos(np.pi * it / max(steps, 1)))  # cosine schedule
+        net.update(lr=float(a))
+        if it % log_every == 0 or it == steps - 1:
+            log.append((it, float(net.loss_acc.item()) / tgt.numel()))
+    net.check_device()
+    return log, time.perf_counter() - t0
+
+
+def _rmse(a, b, mask=None):
+    d = (a - b) if mask is None else (a - b)[mask]
+    return float(np.sqrt(np.mean(d.astype(np.float64) ** 2))) if d.size else 0.0
+
+
+def _iou(a, b, thr=0.05):
+    wa, wb = a > thr, b > thr
+    u = np.logical_or(wa, wb).sum()
+    return float(np.logical_and(wa, wb).sum() / u) if u else 1.0
+
+
+def evaluate_one_call(net: Surrogate, batch: Batch, snaps):
+    """60-s prediction error of the depth over all held-out pairs: network vs persistence."""
+    torch = _torch()
+    T = snaps["h"].shape[0] - 1
+    se_net = se_pers = 0.0
+    n = 0
+    for t in range(T):
+        st = {k: snaps[k][t].clone() for k in ("h", "qx", "qy")}
+        net.advance(batch.state(st["h"], st["qx"], st["qy"]), batch.pins)
+        ref = snaps["h"][t + 1].cpu().numpy()
+        got = st["h"].cpu().numpy()
+        pers = snaps["h"][t].cpu().numpy()
+        se_net += float(np.sum((got.astype(np.float64) - ref) ** 2))
+        se_pers += float(np.sum((pers.astype(np.float64) - ref) ** 2))
+        n += ref.size
+    torch.cuda.synchronize()
+    return {"rmse_depth_net_m": float(np.sqrt(se_net / n)), "rmse_depth_persistence_m": float(np.sqrt(se_pers / n))}
+
+
+def rollout(net: Surrogate, batch: Batch, n_calls: int, h0, qx0, qy0, residual_threshold: float = 1e-3):
+    """Closed-loop surrogate run from (h0, qx0, qy0) over n_calls calls: final state, max-depth
+    maps (over the 60-s states) and, per member, whether the mass-balance residual tripped:
+    |change of inner volume - 60 s x mean edge inflow| > threshold x inner volume, checked at
+    every call (inner cells [2, W-2] x [1, H-2]: the left z condition also sets column 1)."""
+    torch = _torch()
+    st = {"h": h0.clone(), "qx": qx0.clone(), "qy": qy0.clone()}
+    state = batch.state(st["h"], st["qx"], st["qy"])
+    hmax = st["h"].clone()
+    tripped = np.zeros(batch.n, bool)
+    worst = np.zeros(batch.n)
+    dx = 3.0
+    h_host = h0.cpu().numpy()
+    vol = h_host[:, 1:-1, 2:-1].astype(np.float64).sum(axis=(1, 2))
+    # floor of the reference volume: 1 cm of water over 1 % of the inner cells (a dry start
+    # would otherwise make every relative residual infinite)
+    floor = 0.01 * 0.01 * (batch.H - 2) * (batch.W - 3)
+    for c in range(n_calls):
+        f0 = net.edge_flux(st["qx"], st["qy"])
+        dvol = net.advance(state, batch.pins, hmax)
+        f1 = net.edge_flux(st["qx"], st["qy"])
+        dv, a, b = dvol.cpu().numpy(), f0.cpu().numpy(), f1.cpu().numpy()
+        vol = vol + dv
+        rel = np.abs(dv - CALL_S / dx * 0.5 * (a + b)) / np.maximum(vol, floor)
+        worst = np.maximum(worst, rel)
+        tripped |= rel > residual_threshold
+    torch.cuda.synchronize()
+    return st, hmax, tripped, worst
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--members", type=int, default=32, help="training trajectories")
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--hours", type=float, default=1.0, help="simulated length of each training trajectory")
+    ap.add_argument("--steps", type=int, default=400, help="training steps")
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--eval-members", type=int, default=8)
+    ap.add_argument("--screen-members", type=int, default=32)
+    ap.add_argument("--screen-size", type=int, default=512)
+    ap.add_argument("--screen-hours", type=float, default=1.0)
+    ap.add_argument("--out", default="")
+    a = ap.parse_args(argv)
+    torch = _torch()
+    d = tempfile.mkdtemp(prefix="fip_sg_")
+    n_calls = int(round(a.hours * 3600 / CALL_S))
+    res = {"config": vars(a)}
+    # ---- training data from the solver
+    tr = config3_members(d, a.members, a.size, seed=1, duration=a.hours * 3600 + 600)
+    btr = Batch(tr)
+    snaps, _, t_gen = solver_trajectories(tr, n_calls)
+    res["train_data"] = {"pairs": a.members * n_calls, "solver_s": round(t_gen, 2)}
+    # ---- training
+    net = Surrogate(seed=0)
+    log, t_train = train(net, btr, snaps, a.steps, bs=a.batch, lr=a.lr)
+    res["train"] = {"loss_log": log, "seconds": round(t_train, 2), "steps": a.steps,
+                    "ms_per_step": round(1e3 * t_train / max(a.steps, 1), 2)}
+    del snaps
+    torch.cuda.empty_cache()
+    # ---- held-out evaluation
+    ev = config3_members(d, a.eval_members, a.size, seed=2, duration=a.hours * 3600 + 600)
+    bev = Batch(ev)
+    esn, ehmax, _ = solver_trajectories(ev, n_calls)
+    res["eval_one_call"] = evaluate_one_call(net, bev, esn)
+    st, hm, tripped, worst = rollout(net, bev, n_calls, esn["h"][0], esn["qx"][0], esn["qy"][0])
+    ref_h = esn["h"][n_calls].cpu().numpy()
+    got_h = st["h"].cpu().numpy()
+    pers = esn["h"][0].cpu().numpy()
+    res["eval_rollout"] = {"calls": n_calls, "rmse_final_depth_m": _rmse(got_h, ref_h),
+                           "rmse_final_depth_persistence_m": _rmse(pers, ref_h),
+                           "rmse_hmax_m": _rmse(hm.cpu().numpy(), ehmax.cpu().numpy()),
+                           "iou_hmax_5cm": float(np.mean([_iou(hm[i].cpu().numpy(), ehmax[i].cpu().numpy())
+                                                          for i in range(bev.n)])),
+                           "fallback_tripped": int(tripped.sum()), "worst_residual": float(np.max(worst))}
+    del esn
+    torch.cuda.empty_cache()
+    # ---- screening
+    n_sc = int(round(a.screen_hours * 3600 / CALL_S))
+    sc = config3_members(d, a.screen_members, a.screen_size, seed=3, duration=a.screen_hours * 3600)
+    bsc = Batch(sc)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with Ensemble([s.yaml_path for s in sc]) as e:
+        e.step(n_sc * STEPS_PER_CALL)
+        ref_hmax = torch.empty((bsc.n, bsc.H, bsc.W), dtype=torch.float32, device="cuda")
+        e.gather("hmax", ref_hmax)
+    torch.cuda.synchronize()
+    t_solver_all = time.perf_counter() - t0
+    h0 = torch.zeros((bsc.n, bsc.H, bsc.W), dtype=torch.float32, device="cuda")
+    q0 = torch.zeros_like(h0)
+    t0 = time.perf_counter()
+    _, s_hmax, tripped, worst = rollout(net, bsc, n_sc, h0, q0, q0.clone())
+    area = (s_hmax.cpu().numpy() > 0.05).sum(axis=(1, 2))
+    k = max(1, int(round(0.1 * bsc.n)))
+    rerun = set(np.argsort(-area)[:k].tolist()) | set(np.nonzero(tripped)[0].tolist())
+    rerun = sorted(rerun)
+    final = s_hmax.clone()
+    if rerun:
+        with Ensemble([sc[i].yaml_path for i in rerun]) as e:
+            e.step(n_sc * STEPS_PER_CALL)
+            rh = torch.empty((len(rerun), bsc.H, bsc.W), dtype=torch.float32, device="cuda")
+            e.gather("hmax", rh)
+        for j, i in enumerate(rerun):
+            final[i].copy_(rh[j])
+    torch.cuda.synchronize()
+    t_screen = time.perf_counter() - t0
+    fin, ref = final.cpu().numpy(), ref_hmax.cpu().numpy()
+    res["screening"] = {"members": bsc.n, "size": bsc.H, "hours": a.screen_hours, "rerun": len(rerun),
+                        "fallback_tripped": int(tripped.sum()), "wall_s_screened": round(t_screen, 2),
+                        "wall_s_batched_solver_all": round(t_solver_all, 2),
+                        "speedup": round(t_solver_all / max(t_screen, 1e-9), 3),
+                        "rmse_hmax_m": _rmse(fin, ref), "iou_5cm": float(np.mean([_iou(fin[i], ref[i]) for i in range(bsc.n)])),
+                        "rmse_hmax_surrogate_only_m": _rmse(s_hmax.cpu().numpy(), ref)}
+    if a.out:
+        np.save(a.out, net.params())
+    print(json.dumps(res), flush=True)
+    return res
+
+
+if __name__ == "__main__":
+    main()

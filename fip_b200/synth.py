@@ -158,7 +158,7 @@ def scenario0(outdir: str, W: int = 1024, H: int = 1024, dx: float = 3.0, dt: fl
         ]
     ypath = os.path.join(outdir, f"{name}.yml")
     write_yaml(ypath, cfg)
-    return Scenario(ypath, W, H, terr, info={"zbc": zbc, "bc_rows": bc_rows})
+    return Scenario(ypath, W, H, terr, info={"zbc": zbc, "bc_rows": bc_rows, "kst": kst, "level_add": level_add})
 
 
 def fbm(W: int, H: int, hurst: float, seed: int) -> np.ndarray:

@@ -53,11 +53,12 @@ int fip_sg_adamw(float* p, const float* g, float* m, float* v, long long n, floa
  * convolution, wd [l][9][in][out] with reversed taps for the input gradient. */
 int fip_sg_cast_weights(const float* p, int n_layers, void* wf, void* wd, void* stream);
 /* One surrogate call: h = max(0, h + 0.5 * pred0), qx += pred1, qy += pred2 (no-data cells kept);
- * dvol[n] += change of the depth sum over the inner cells [1, W-2] x [1, H-2] of image n
- * (H * W >= 256). */
+ * dvol[n] += change of the depth sum over the inner cells [2, W-2] x [1, H-2] of image n
+ * (H * W >= 256); hmax (may be NULL) = max(hmax, new h). */
 int fip_sg_apply(const float* pred, int N, int H, int W, const float* terrain, float no_value, float* h, float* qx,
-                 float* qy, double* dvol, void* stream);
-/* flux[n] = net discharge per unit width into the inner cells of image n. */
+                 float* qy, double* dvol, float* hmax, void* stream);
+/* flux[n] = net discharge per unit width into the inner cells [2, W-2] x [1, H-2] of image n
+ * (through qx[:, 1], qx[:, W-2], qy[0, :], qy[H-2, :]). */
 int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, void* stream);
 
 /* Cells fixed by boundary conditions: mask bit 0 sets h, bit 1 qx, bit 2 qy to the given values. */
