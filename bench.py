@@ -16,6 +16,12 @@ timed graph. With N > 1 (torchrun) every rank runs an independent replica ("repl
 --impl reference times the reference's algorithm on the host cores: the reference's path is CUDA
 only, so its CPU stand-in is the FP64 restatement (oracle port) with all host threads, on a
 bounded row band of the same scenario.
+
+Two informational objects ride on the same line (N = 1 only): `ensemble` (64 scenarios of
+W, H ~ U[256, 2048] as one batched ensemble, every tile computed, autotuned tile shape, against
+the same scenarios run one at a time, plus a flooded state with dry-tile skipping) and
+`surrogate` (the tcgen05 convolutions of the learned surrogate against the measured bf16 GEMM
+peak, and a reduced train / evaluate / screen run of fip_b200.surrogate_run).
 """
 from __future__ import annotations
 
@@ -220,6 +226,36 @@ def ensemble_measure(args, local_rank):
     return out
 
 
+def bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def surrogate_measure(args):
+    """Learned surrogate: throughput of its tcgen05 convolutions (32 x 512 x 512 x 64, CUDA
+    events) against the measured bf16 GEMM peak, and a reduced train / evaluate / screen run of
+    fip_b200.surrogate_run (trajectories from the batched solver; see that module)."""
+    from fip_b200 import surrogate_run
+    from fip_b200.surrogate import bench_convs
+
+    peak, kind = bf16_peak()
+    conv = bench_convs(32, 512, 512, 10)
+    out = {"conv_32x512x512": {k: {"ms": round(v["ms"], 4), "tflops": round(v["tflops"], 1),
+                                   "frac_of_bf16_peak": round(v["tflops"] / peak, 3)} for k, v in conv.items()},
+           "bf16_peak_tflops": peak, "peak_source": f"{kind} (MEASURED_PEAKS.json bf16_tflops)"}
+    res = surrogate_run.main(["--members", str(args.sg_members), "--size", str(args.sg_size), "--hours",
+                              str(args.sg_hours), "--steps", str(args.sg_steps), "--batch", str(args.sg_batch),
+                              "--eval-members", "4", "--screen-members", str(args.sg_members), "--screen-size",
+                              str(args.sg_size), "--screen-hours", str(args.sg_hours)], emit=False)
+    out["pipeline"] = {k: v for k, v in res.items() if k != "config"}
+    out["pipeline"]["config"] = {"members": args.sg_members, "size": args.sg_size, "hours": args.sg_hours,
+                                 "train_steps": args.sg_steps, "batch": args.sg_batch}
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -326,6 +362,12 @@ def run_gpu(args, rank, world, local_rank):
             ens = ensemble_measure(args, local_rank)
         except Exception as exc:  # reported in the line; the headline stands on its own
             ens = {"error": f"{type(exc).__name__}: {exc}"}
+    sgm = None
+    if world == 1 and args.sg_members > 0:
+        try:
+            sgm = surrogate_measure(args)
+        except Exception as exc:
+            sgm = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
         base = None
         if world == 1 and not args.no_cpu_baseline:
@@ -342,7 +384,7 @@ def run_gpu(args, rank, world, local_rank):
                         "d2h_bytes_per_step": 3 * cells * 4,
                         "note": f"each e2e step = upload h,qx,qy from pinned host + {inner} solver steps + download"},
                 "gpu_launches": 2 * args.steps, "roofline": roof, "clocks": clocks,
-                "cpu_baseline": base, "active_tiles": active, "ensemble": ens}
+                "cpu_baseline": base, "active_tiles": active, "ensemble": ens, "surrogate": sgm}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -366,6 +408,11 @@ def main():
     ap.add_argument("--ens-steps", type=int, default=200)
     ap.add_argument("--ens-seq-steps", type=int, default=20)
     ap.add_argument("--ens-spinup", type=int, default=3000)
+    ap.add_argument("--sg-members", type=int, default=16, help="surrogate measurement (0: skip)")
+    ap.add_argument("--sg-size", type=int, default=512)
+    ap.add_argument("--sg-hours", type=float, default=0.5)
+    ap.add_argument("--sg-steps", type=int, default=300)
+    ap.add_argument("--sg-batch", type=int, default=16)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

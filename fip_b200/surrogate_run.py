@@ -206,7 +206,7 @@ def rollout(net: Surrogate, batch: Batch, n_calls: int, h0, qx0, qy0, residual_t
     return st, hmax, tripped, worst
 
 
-def main(argv=None):
+def main(argv=None, emit: bool = True):
     ap = argparse.ArgumentParser()
     ap.add_argument("--members", type=int, default=32, help="training trajectories")
     ap.add_argument("--size", type=int, default=512)
@@ -292,7 +292,8 @@ def main(argv=None):
                         "rmse_hmax_surrogate_only_m": _rmse(s_hmax.cpu().numpy(), ref)}
     if a.out:
         np.save(a.out, net.params())
-    print(json.dumps(res), flush=True)
+    if emit:
+        print(json.dumps(res), flush=True)
     return res
 
 
