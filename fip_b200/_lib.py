@@ -116,15 +116,15 @@ def lib():
         L.fip_ensemble_render.restype = ctypes.c_int
         L.fip_ensemble_gather.argtypes = [vp, ip, vp]
         f32, ll = ctypes.c_float, ctypes.c_longlong
-        L.fip_sg_conv3x3.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, vp, vp]
-        L.fip_sg_conv3x3_wgrad.argtypes = [vp, vp, vp, ip, ip, ip, vp, vp]
+        L.fip_sg_conv3x3.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, ip, vp, vp]
+        L.fip_sg_conv3x3_wgrad.argtypes = [vp, vp, vp, ip, ip, ip, ip, vp, vp]
         L.fip_sg_pack_input.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, f32, vp, vp]
         L.fip_sg_target.argtypes = [vp, vp, vp, vp, vp, vp, vp, ll, f32, vp, vp]
-        L.fip_sg_loss.argtypes = [vp, vp, ip, ip, ip, vp, vp, vp]
+        L.fip_sg_loss.argtypes = [vp, vp, ip, ip, ip, f32, vp, vp, vp, vp]
         L.fip_sg_bias_grad.argtypes = [vp, ll, vp, vp]
         L.fip_sg_adamw.argtypes = [vp, vp, vp, vp, ll, f32, f32, f32, f32, f32, ip, vp]
         L.fip_sg_cast_weights.argtypes = [vp, ip, vp, vp, vp]
-        L.fip_sg_apply.argtypes = [vp, ip, ip, ip, vp, f32, vp, vp, vp, vp, vp, vp]
+        L.fip_sg_apply.argtypes = [vp, ip, ip, ip, f32, vp, f32, vp, vp, vp, vp, vp, vp]
         L.fip_sg_edge_flux.argtypes = [vp, vp, ip, ip, ip, vp, vp]
         L.fip_sg_pin.argtypes = [vp, vp, vp, vp, ll, vp, vp, vp, vp]
         L.fip_sg_pin.restype = ctypes.c_int

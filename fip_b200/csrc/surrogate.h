@@ -24,12 +24,19 @@ namespace sg {
 constexpr float kFeatZ = 0.1f;   // terrain / level relative to the image's mean terrain, per metre
 constexpr float kFeatK = 0.025f; // Strickler coefficient
 constexpr float kFeatQ = 0.2f;   // discharge per unit width, per m2/s
-constexpr float kOutZ = 0.5f;    // depth change of one call, metres per output unit
+constexpr float kOutZ = 0.5f;    // depth change of one call, metres per target unit
 constexpr float kOutQ = 1.0f;    // discharge change of one call, m2/s per output unit
+constexpr float kOutF = 1.0f;    // mean face discharge over one call, m2/s per output unit
+constexpr float kCallS = 60.0f;  // simulated seconds of one call
 constexpr size_t kLayerParams = (size_t)9 * 64 * 64 + 64;  // weights then biases of one conv layer
 
+// zero border around every image of a network tensor: taps of dilation up to kPad stay inside it
+constexpr int kPad = 8;
+constexpr int kMaxDil = 8;
+
 struct ConvShape {
-  int N, H, W;  // images and interior size; tensors hold N x (H + 2) x (W + 2) pixels x 64 channels
+  int N, H, W;  // images and interior size; tensors hold N x (H + 2 kPad) x (W + 2 kPad) pixels x 64 channels
+  int dil;      // dilation of the 3x3 kernel: tap (dy, dx) reads (y + dil * dy, x + dil * dx)
 };
 
 // 3x3 convolution, 64 -> 64 channels, weights bf16 [9 taps][64 out][64 in] (tap = (dy + 1) * 3 + dx + 1).
@@ -50,14 +57,14 @@ cudaError_t pack_input(const float* h, const float* qx, const float* qy, const f
                        const float* zref, int N, int H, int W, float no_value, __nv_bfloat16* out, cudaStream_t s);
 cudaError_t make_target(const float* h0, const float* qx0, const float* qy0, const float* h1, const float* qx1,
                         const float* qy1, const float* terr, size_t total, float no_value, float* tgt, cudaStream_t s);
-cudaError_t loss_and_grad(const float* pred, const float* tgt, int N, int H, int W, __nv_bfloat16* grad, double* loss,
-                          cudaStream_t s);
+cudaError_t loss_and_grad(const float* pred, const float* tgt, int N, int H, int W, float dx, float* scratch,
+                          __nv_bfloat16* grad, double* loss, cudaStream_t s);
 cudaError_t bias_grad(const __nv_bfloat16* g, size_t n_pix, float* db, cudaStream_t s);
 cudaError_t adamw(float* p, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2, float eps,
                   float wd, int step, cudaStream_t s);
 cudaError_t cast_weights(const float* p, int n_layers, __nv_bfloat16* wf, __nv_bfloat16* wd, cudaStream_t s);
-cudaError_t apply_update(const float* pred, int N, int H, int W, const float* terr, float no_value, float* h, float* qx,
-                         float* qy, double* dvol, float* hmax, cudaStream_t s);
+cudaError_t apply_update(const float* pred, int N, int H, int W, float dx, const float* terr, float no_value, float* h,
+                         float* qx, float* qy, double* dvol, float* hmax, cudaStream_t s);
 cudaError_t edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, cudaStream_t s);
 cudaError_t pin_cells(const unsigned char* mask, const float* hv, const float* qxv, const float* qyv, size_t total,
                       float* h, float* qx, float* qy, cudaStream_t s);

@@ -32,7 +32,7 @@ float* g_part[64] = {};
 extern "C" {
 
 int fip_sg_conv3x3(const void* in, const void* w, const float* bias, const void* res, const void* mask, void* out,
-                   int N, int H, int W, int epi, int* dev_err, void* stream) {
+                   int N, int H, int W, int dilation, int epi, int* dev_err, void* stream) {
   if (!in || !w || !out || N <= 0 || H <= 0 || W <= 0) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: bad argument");
   if (epi < FIP_SG_EPI_BIAS_RELU || epi > FIP_SG_EPI_PLAIN) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: unknown epilogue");
   if ((epi == FIP_SG_EPI_BIAS_RES_RELU || epi == FIP_SG_EPI_RES_MASK) && !res)
@@ -41,15 +41,18 @@ int fip_sg_conv3x3(const void* in, const void* w, const float* bias, const void*
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: this epilogue needs mask");
   if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(out)) & 15u)
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: tensors must be 16-byte aligned");
-  if ((long long)N * (H + 2) * (W + 2) >= (1LL << 31)) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: too many pixels");
-  fip::sg::ConvShape s{N, H, W};
+  if ((long long)N * (H + 2 * fip::sg::kPad) * (W + 2 * fip::sg::kPad) >= (1LL << 31))
+    return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: too many pixels");
+  if (dilation < 1 || dilation > fip::sg::kMaxDil) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: dilation must be 1..8");
+  fip::sg::ConvShape s{N, H, W, dilation};
   return sg_cuda(fip::sg::conv3x3(s, static_cast<const __nv_bfloat16*>(in), static_cast<const __nv_bfloat16*>(w), bias,
                                   static_cast<const __nv_bfloat16*>(res), static_cast<const __nv_bfloat16*>(mask), out, epi,
                                   dev_err, static_cast<cudaStream_t>(stream)),
                  "fip_sg_conv3x3");
 }
 
-int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H, int W, int* dev_err, void* stream) {
+int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H, int W, int dilation, int* dev_err,
+                         void* stream) {
   if (!x || !dy || !dw || N <= 0 || H <= 0 || W <= 0) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: bad argument");
   if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(dy)) & 15u)
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: tensors must be 16-byte aligned");
@@ -66,7 +69,8 @@ int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H,
     }
     part = g_part[dev];
   }
-  fip::sg::ConvShape s{N, H, W};
+  if (dilation < 1 || dilation > fip::sg::kMaxDil) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: dilation must be 1..8");
+  fip::sg::ConvShape s{N, H, W, dilation};
   return sg_cuda(fip::sg::conv3x3_wgrad(s, static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy),
                                         part, dw, dev_err, static_cast<cudaStream_t>(stream)),
                  "fip_sg_conv3x3_wgrad");
@@ -91,9 +95,12 @@ int fip_sg_target(const float* h0, const float* qx0, const float* qy0, const flo
                  "fip_sg_target");
 }
 
-int fip_sg_loss(const float* pred, const float* tgt, int N, int H, int W, void* grad, double* loss, void* stream) {
-  if (!pred || !tgt || !grad || !loss || N <= 0 || H <= 0 || W <= 0) return sg_fail(FIP_ERR_ARG, "fip_sg_loss: bad argument");
-  return sg_cuda(fip::sg::loss_and_grad(pred, tgt, N, H, W, static_cast<__nv_bfloat16*>(grad), loss, SG_S), "fip_sg_loss");
+int fip_sg_loss(const float* pred, const float* tgt, int N, int H, int W, float dx, float* scratch, void* grad,
+                double* loss, void* stream) {
+  if (!pred || !tgt || !grad || !loss || !scratch || N <= 0 || H <= 0 || W <= 0 || !(dx > 0.f))
+    return sg_fail(FIP_ERR_ARG, "fip_sg_loss: bad argument");
+  return sg_cuda(fip::sg::loss_and_grad(pred, tgt, N, H, W, dx, scratch, static_cast<__nv_bfloat16*>(grad), loss, SG_S),
+                 "fip_sg_loss");
 }
 
 int fip_sg_bias_grad(const void* g, long long n_pix, float* db, void* stream) {
@@ -114,11 +121,11 @@ int fip_sg_cast_weights(const float* p, int n_layers, void* wf, void* wd, void* 
                  "fip_sg_cast_weights");
 }
 
-int fip_sg_apply(const float* pred, int N, int H, int W, const float* terrain, float no_value, float* h, float* qx,
-                 float* qy, double* dvol, float* hmax, void* stream) {
-  if (!pred || !terrain || !h || !qx || !qy || !dvol || N <= 0 || (long long)H * W < 256)
+int fip_sg_apply(const float* pred, int N, int H, int W, float dx, const float* terrain, float no_value, float* h,
+                 float* qx, float* qy, double* dvol, float* hmax, void* stream) {
+  if (!pred || !terrain || !h || !qx || !qy || !dvol || N <= 0 || (long long)H * W < 256 || !(dx > 0.f))
     return sg_fail(FIP_ERR_ARG, "fip_sg_apply: bad argument (images of at least 256 cells)");
-  return sg_cuda(fip::sg::apply_update(pred, N, H, W, terrain, no_value, h, qx, qy, dvol, hmax, SG_S), "fip_sg_apply");
+  return sg_cuda(fip::sg::apply_update(pred, N, H, W, dx, terrain, no_value, h, qx, qy, dvol, hmax, SG_S), "fip_sg_apply");
 }
 
 int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, void* stream) {

@@ -1,10 +1,10 @@
 // BF16 3x3 convolutions of the learned surrogate on the 5th-generation tensor cores (tcgen05).
 //
-// Activations are NHWC bf16 with 64 channels and a one-pixel zero border around each image:
-// row p of the [N * (H + 2) * (W + 2)][64] matrix is one (padded) pixel, 128 bytes. With that
-// layout a 3x3 convolution is an implicit GEMM whose nine taps are plain row shifts of the
-// activation matrix (tap (dy, dx) reads row p + dy * (W + 2) + dx), so every operand tile is one
-// TMA box:
+// Activations are NHWC bf16 with 64 channels and a zero border of kPad pixels around each
+// image: row p of the [N * (H + 2 kPad) * (W + 2 kPad)][64] matrix is one (padded) pixel, 128
+// bytes. With that layout a 3x3 convolution of dilation d <= kPad is an implicit GEMM whose nine
+// taps are plain row shifts of the activation matrix (tap (dy, dx) reads row
+// p + d * (dy * Wp + dx), Wp = W + 2 kPad), so every operand tile is one TMA box:
 //
 //   forward / dgrad   D[128 pixels][64 out] += sum over 9 taps of
 //                     A_tap[128 pixels][64 in] (K-major, rows shifted) x B_tap[64 out][64 in]^T
@@ -35,9 +35,8 @@ constexpr int C = 64;                   // channels of every activation tensor
 constexpr int BM = 128;                 // pixels per forward tile (MMA M)
 constexpr int kTapBytes = C * C * 2;    // 8 KB: one tap of the weights, 64 x 64 bf16
 constexpr int kWBytes = 9 * kTapBytes;  // 72 KB
-constexpr int kSlabRows = 136;         // a tile's 128 rows plus the 2 rows the dx shifts reach, rounded to 8
-constexpr int kSlabBytes = kSlabRows * C * 2;  // 17 KB of one dy slab
-constexpr int kSlabStride = 18 * 1024;  // slabs start on 1024-byte boundaries (swizzle pattern)
+// one slab per kernel row: a tile's 128 rows plus the 2 * dilation rows its dx shifts reach
+constexpr int kSlabStride = 18 * 1024;  // slabs start on 1024-byte boundaries (swizzle pattern); <= 144 rows
 constexpr int kStages = 6;
 constexpr int kThreads = 192;           // warp 0: TMA, warp 1: MMA + TMEM owner, warps 2-5: epilogue
 constexpr unsigned long long kWaitNs = 2000000000ull;
@@ -157,6 +156,7 @@ struct FwdArgs {
   const __nv_bfloat16* mask;// ReLU mask source (> 0 passes)
   void* out;                // bf16 [n_pix][64], or f32 [n_pix][4] (EPI_HEAD)
   int n_pix, Hp, Wp;        // padded pixel count, padded image height / width
+  int dil, slab_rows;       // dilation, rows of one slab (128 + 2 dil)
   int n_tiles;
   int* err;
 };
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ok = true;
       for (int tile = blockIdx.x; ok && tile < a.n_tiles; tile += gridDim.x) {
         const int p0 = tile * BM;
-        for (int r = 0; r < 3; ++r, ++it) {  // rows p0 + dy * Wp - 1 .. + 134 serve the taps (dy, -1..1)
+        for (int r = 0; r < 3; ++r, ++it) {  // rows from p0 + dil * (dy * Wp - 1) serve the taps (dy, -1..1)
           const uint32_t st = it % kStages, ph = (it / kStages) & 1u;
           if (!mbar_wait(&empty_bar[st], ph ^ 1u, &s_abort)) {
             record(a.err, 1);
@@ -221,8 +221,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           const int dy = r - 1;
-          mbar_expect_tx(&full_bar[st], kSlabBytes);
-          tma_2d(s_a + st * kSlabStride, &tm_act, 0, p0 + dy * Wp - 1, &full_bar[st]);
+          mbar_expect_tx(&full_bar[st], (uint32_t)a.slab_rows * C * 2);
+          tma_2d(s_a + st * kSlabStride, &tm_act, 0, p0 + a.dil * (dy * Wp - 1), &full_bar[st]);
         }
       }
     }
@@ -255,8 +255,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           tc_fence_after();
           const uint32_t slab = smem_u32(s_a + st * kSlabStride);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {  // tap (dy, dx = c - 1): the slab from row c on
-            const uint32_t sa = slab + 128 * c, sb = smem_u32(s_w + (3 * r + c) * kTapBytes);
+          for (int c = 0; c < 3; ++c) {  // tap (dy, dx = c - 1): the slab from row c * dil on
+            const uint32_t sa = slab + 128 * c * a.dil, sb = smem_u32(s_w + (3 * r + c) * kTapBytes);
 #pragma unroll
             for (int k = 0; k < 4; ++k)
               tc_mma(d, sdesc(sa + 32 * k, 16, 1024), sdesc(sb + 32 * k, 16, 1024), idesc, (r | c | k) ? 1u : 0u);
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int p = tile * BM + row;
       if (p >= a.n_pix) continue;
       const int xx = p % Wp, yy = (p / Wp) % a.Hp;
-      const bool interior = xx >= 1 && xx <= Wp - 2 && yy >= 1 && yy <= a.Hp - 2;
+      const bool interior = xx >= kPad && xx < Wp - kPad && yy >= kPad && yy < a.Hp - kPad;
       if (EPI == EPI_HEAD) {
         float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
         if (interior) o = make_float4(v[0] + s_bias[0], v[1] + s_bias[1], v[2] + s_bias[2], v[3] + s_bias[3]);
@@ -359,7 +359,7 @@ constexpr int kWgStages = 2;
 
 struct WgArgs {
   float* part;  // [gridDim.x][9][64][64]
-  int n_pix, Wp;
+  int n_pix, Wp, dil;
   int n_chunks;
   int* err;
 };
@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int j = 0; j < 10; ++j) {
           const int t = j < 9 ? j : 8;
           const int dy = t / 3 - 1, dx = t % 3 - 1;
-          tma_2d(s + j * kWgAtom, &tm_x, 0, p0 + dy * a.Wp + dx, &full_bar[st]);
+          tma_2d(s + j * kWgAtom, &tm_x, 0, p0 + a.dil * (dy * a.Wp + dx), &full_bar[st]);
         }
         tma_2d(s + 10 * kWgAtom, &tm_dy, 0, p0, &full_bar[st]);
       }
@@ -525,17 +525,21 @@ cudaError_t conv3x3(const ConvShape& s, const __nv_bfloat16* in, const __nv_bflo
                     cudaStream_t stream) {
   std::string derr;
   if (!drv::load(&derr)) return cudaErrorInitializationError;
-  const int n_pix = s.N * (s.H + 2) * (s.W + 2);
+  if (s.dil < 1 || s.dil > kMaxDil) return cudaErrorInvalidValue;
+  const int n_pix = s.N * (s.H + 2 * kPad) * (s.W + 2 * kPad);
+  const int slab_rows = BM + 2 * s.dil;
   CUtensorMap tm_a, tm_w;
-  if (encode_act_map(&tm_a, in, n_pix, kSlabRows) || encode_act_map(&tm_w, w, 9 * C, C)) return cudaErrorInvalidValue;
+  if (encode_act_map(&tm_a, in, n_pix, slab_rows) || encode_act_map(&tm_w, w, 9 * C, C)) return cudaErrorInvalidValue;
   FwdArgs a;
   a.bias = bias;
   a.res = res;
   a.mask = mask;
   a.out = out;
   a.n_pix = n_pix;
-  a.Hp = s.H + 2;
-  a.Wp = s.W + 2;
+  a.Hp = s.H + 2 * kPad;
+  a.Wp = s.W + 2 * kPad;
+  a.dil = s.dil;
+  a.slab_rows = slab_rows;
   a.n_tiles = (n_pix + BM - 1) / BM;
   a.err = err;
   const int smem = kWBytes + kStages * kSlabStride + 1024;
@@ -570,13 +574,15 @@ cudaError_t conv3x3_wgrad(const ConvShape& s, const __nv_bfloat16* x, const __nv
                           int* err, cudaStream_t stream) {
   std::string derr;
   if (!drv::load(&derr)) return cudaErrorInitializationError;
-  const int n_pix = s.N * (s.H + 2) * (s.W + 2);
+  if (s.dil < 1 || s.dil > kMaxDil) return cudaErrorInvalidValue;
+  const int n_pix = s.N * (s.H + 2 * kPad) * (s.W + 2 * kPad);
   CUtensorMap tm_x, tm_dy;
   if (encode_act_map(&tm_x, x, n_pix, kWgChunk) || encode_act_map(&tm_dy, dy, n_pix, kWgChunk)) return cudaErrorInvalidValue;
   WgArgs a;
   a.part = part;
   a.n_pix = n_pix;
-  a.Wp = s.W + 2;
+  a.Wp = s.W + 2 * kPad;
+  a.dil = s.dil;
   a.n_chunks = (n_pix + kWgChunk - 1) / kWgChunk;
   a.err = err;
   const int smem = kWgStages * kWgStageBytes + 1024;

@@ -2,9 +2,15 @@
 // its gradient, bias gradients, AdamW with the bf16 weight layouts of the forward and backward
 // convolutions, the surrogate's state update and its mass-balance residual.
 //
+// The network's four outputs per cell are the mean discharges through its east and north faces
+// over the call (Fx, Fy, per unit width) and the changes of qx and qy. The depth changes by the
+// discrete continuity equation, dh = -(T / dx) (Fx - Fx_west + Fy - Fy_south), so water only
+// moves between neighbours or through the domain edge: the surrogate conserves mass by
+// construction (up to the clamp of negative depths).
+//
 // Grids are fp32 [N][H][W] (one image per scenario, row 0 = southern edge); network tensors are
-// NHWC bf16 [N][H+2][W+2][64] with a zero border (see surrogate_conv.cu), the network output is
-// fp32 [N][H+2][W+2][4]. Feature and output scales are fixed constants (kFeat*, kOut*).
+// NHWC bf16 [N][H + 2 kPad][W + 2 kPad][64] with a zero border (see surrogate_conv.cu), the
+// network output is fp32 [N][H + 2 kPad][W + 2 kPad][4]. Feature and output scales are fixed constants (kFeat*, kOut*).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -17,7 +23,13 @@ namespace sg {
 namespace {
 
 __device__ __forceinline__ size_t ppix(int n, int y, int x, int H, int W) {  // padded pixel of interior (y, x)
-  return ((size_t)n * (H + 2) + (y + 1)) * (size_t)(W + 2) + (x + 1);
+  return ((size_t)n * (H + 2 * kPad) + (y + kPad)) * (size_t)(W + 2 * kPad) + (x + kPad);
+}
+
+// depth change of cell (y, x) from the face discharges (the border pixels of pred are zero, so
+// faces outside the image carry nothing); c = T / dx * kOutF
+__device__ __forceinline__ float dh_of(const float* __restrict__ pred, size_t p, int Wp, float c) {
+  return -c * ((pred[p * 4 + 0] - pred[(p - 1) * 4 + 0]) + (pred[p * 4 + 1] - pred[(p - Wp) * 4 + 1]));
 }
 
 // features: 0 terrain - zref, 1 kSt, 2 level - zref, 3 qx, 4 qy, 5 wet (h > 1 cm); 6..63 zero
@@ -64,9 +76,10 @@ __global__ void target_kernel(const float* __restrict__ h0, const float* __restr
   tgt[3 * i + 2] = valid ? (qy1[i] - qy0[i]) * (1.f / kOutQ) : 0.f;
 }
 
-// loss = mean over interior pixels and 3 outputs of (pred - target)^2; grad as bf16 [pix][64]
-__global__ void loss_kernel(const float* __restrict__ pred, const float* __restrict__ tgt, int N, int H, int W,
-                            float inv_count, __nv_bfloat16* __restrict__ grad, double* __restrict__ loss) {
+// loss = mean over interior cells and 3 outputs of the squared errors of (dh / kOutZ, dqx, dqy)
+// against the target. Pass 1: the loss and e[i] = d loss / d(dh / kOutZ) per cell.
+__global__ void loss_pass1_kernel(const float* __restrict__ pred, const float* __restrict__ tgt, int N, int H, int W,
+                                  float c, float inv_count, float* __restrict__ e, double* __restrict__ loss) {
   __shared__ double red[256];
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t total = (size_t)N * H * W;
@@ -75,16 +88,11 @@ __global__ void loss_kernel(const float* __restrict__ pred, const float* __restr
     const int n = (int)(i / ((size_t)H * W));
     const int y = (int)((i / W) % H), x = (int)(i % W);
     const size_t p = ppix(n, y, x, H, W);
-    float g[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int c = 0; c < 3; ++c) {
-      const float d = pred[p * 4 + c] - tgt[3 * i + c];
-      acc += (double)d * d;
-      g[c] = 2.f * d * inv_count;
-    }
-    uint4 v;
-    __nv_bfloat162* pv = reinterpret_cast<__nv_bfloat162*>(&v);
-    for (int k = 0; k < 4; ++k) pv[k] = __floats2bfloat162_rn(g[2 * k], g[2 * k + 1]);
-    reinterpret_cast<uint4*>(grad + p * 64)[0] = v;
+    const float d0 = dh_of(pred, p, W + 2 * kPad, c) * (1.f / kOutZ) - tgt[3 * i + 0];
+    const float d1 = pred[p * 4 + 2] - tgt[3 * i + 1];
+    const float d2 = pred[p * 4 + 3] - tgt[3 * i + 2];
+    acc = (double)d0 * d0 + (double)d1 * d1 + (double)d2 * d2;
+    e[i] = 2.f * d0 * inv_count;
   }
   red[threadIdx.x] = acc;
   __syncthreads();
@@ -93,6 +101,32 @@ __global__ void loss_kernel(const float* __restrict__ pred, const float* __restr
     __syncthreads();
   }
   if (threadIdx.x == 0) atomicAdd(loss, red[0]);
+}
+
+// Pass 2: output gradient as bf16 [pix][64] (channels 0..3). Fx[y][x] enters dh of (y, x) with
+// -c and of (y, x + 1) with +c; Fy[y][x] enters (y, x) and (y + 1, x) likewise.
+__global__ void loss_pass2_kernel(const float* __restrict__ pred, const float* __restrict__ tgt, int N, int H, int W,
+                                  float c, float inv_count, const float* __restrict__ e,
+                                  __nv_bfloat16* __restrict__ grad) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t total = (size_t)N * H * W;
+  if (i >= total) return;
+  const int y = (int)((i / W) % H), x = (int)(i % W);
+  const int n = (int)(i / ((size_t)H * W));
+  const size_t p = ppix(n, y, x, H, W);
+  const float cz = c * (1.f / kOutZ);
+  const float e0 = e[i];
+  const float ee = x + 1 < W ? e[i + 1] : 0.f;
+  const float en = y + 1 < H ? e[i + W] : 0.f;
+  float g[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  g[0] = cz * (ee - e0);
+  g[1] = cz * (en - e0);
+  g[2] = 2.f * (pred[p * 4 + 2] - tgt[3 * i + 1]) * inv_count;
+  g[3] = 2.f * (pred[p * 4 + 3] - tgt[3 * i + 2]) * inv_count;
+  uint4 v;
+  __nv_bfloat162* pv = reinterpret_cast<__nv_bfloat162*>(&v);
+  for (int k = 0; k < 4; ++k) pv[k] = __floats2bfloat162_rn(g[2 * k], g[2 * k + 1]);
+  reinterpret_cast<uint4*>(grad + p * 64)[0] = v;
 }
 
 // db[c] += sum over pixels of g[p][c] (border pixels are zero); 64 channels x pixel slices
@@ -138,12 +172,13 @@ __global__ void cast_weights_kernel(const float* __restrict__ p, int n_layers, _
   wd[l * per + ((size_t)(8 - t) * 64 + c) * 64 + o] = b;
 }
 
-// state update of one surrogate call: h += dz (clamped at 0), qx += dqx, qy += dqy; no-data
-// cells keep their values. dvol[n] += volume change (depth sum) of image n's inner cells;
-// hmax (optional) = max(hmax, new depth).
-__global__ void apply_kernel(const float* __restrict__ pred, int N, int H, int W, const float* __restrict__ terr,
-                             float no_value, float* __restrict__ h, float* __restrict__ qx, float* __restrict__ qy,
-                             double* __restrict__ dvol, float* __restrict__ hmax) {
+// state update of one surrogate call: h += dh of the face discharges (clamped at 0), qx += dqx,
+// qy += dqy; no-data cells keep their values. dvol[n] += volume change (depth sum) of image n's
+// inner cells; hmax (optional) = max(hmax, new depth).
+__global__ void apply_kernel(const float* __restrict__ pred, int N, int H, int W, float c,
+                             const float* __restrict__ terr, float no_value, float* __restrict__ h,
+                             float* __restrict__ qx, float* __restrict__ qy, double* __restrict__ dvol,
+                             float* __restrict__ hmax) {
   __shared__ double red[2][256];
   __shared__ int s_n0;
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -157,11 +192,11 @@ __global__ void apply_kernel(const float* __restrict__ pred, int N, int H, int W
     if (terr[i] != no_value) {
       const size_t p = ppix(n, y, x, H, W);
       const float h0 = h[i];
-      const float h1 = fmaxf(0.f, h0 + pred[p * 4 + 0] * kOutZ);
+      const float h1 = fmaxf(0.f, h0 + dh_of(pred, p, W + 2 * kPad, c));
       h[i] = h1;
       if (hmax) hmax[i] = fmaxf(hmax[i], h1);
-      qx[i] += pred[p * 4 + 1] * kOutQ;
-      qy[i] += pred[p * 4 + 2] * kOutQ;
+      qx[i] += pred[p * 4 + 2] * kOutQ;
+      qy[i] += pred[p * 4 + 3] * kOutQ;
       // volume of the cells only the continuity equation updates (a z condition on the left
       // edge also sets column 1): its change must match the discharge through the faces around
       if (x >= 2 && x <= W - 2 && y >= 1 && y <= H - 2) dv = (double)h1 - (double)h0;
@@ -246,10 +281,13 @@ cudaError_t make_target(const float* h0, const float* qx0, const float* qy0, con
   return cudaGetLastError();
 }
 
-cudaError_t loss_and_grad(const float* pred, const float* tgt, int N, int H, int W, __nv_bfloat16* grad, double* loss,
-                          cudaStream_t s) {
+cudaError_t loss_and_grad(const float* pred, const float* tgt, int N, int H, int W, float dx, float* scratch,
+                          __nv_bfloat16* grad, double* loss, cudaStream_t s) {
   const size_t total = (size_t)N * H * W;
-  loss_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(pred, tgt, N, H, W, 1.f / (3.f * (float)total), grad, loss);
+  const float c = kCallS / dx * kOutF, inv = 1.f / (3.f * (float)total);
+  const unsigned blocks = (unsigned)((total + 255) / 256);
+  loss_pass1_kernel<<<blocks, 256, 0, s>>>(pred, tgt, N, H, W, c, inv, scratch, loss);
+  loss_pass2_kernel<<<blocks, 256, 0, s>>>(pred, tgt, N, H, W, c, inv, scratch, grad);
   return cudaGetLastError();
 }
 
@@ -271,10 +309,11 @@ cudaError_t cast_weights(const float* p, int n_layers, __nv_bfloat16* wf, __nv_b
   return cudaGetLastError();
 }
 
-cudaError_t apply_update(const float* pred, int N, int H, int W, const float* terr, float no_value, float* h, float* qx,
-                         float* qy, double* dvol, float* hmax, cudaStream_t s) {
+cudaError_t apply_update(const float* pred, int N, int H, int W, float dx, const float* terr, float no_value, float* h,
+                         float* qx, float* qy, double* dvol, float* hmax, cudaStream_t s) {
   const size_t total = (size_t)N * H * W;
-  apply_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(pred, N, H, W, terr, no_value, h, qx, qy, dvol, hmax);
+  apply_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(pred, N, H, W, kCallS / dx * kOutF, terr, no_value, h,
+                                                                qx, qy, dvol, hmax);
   return cudaGetLastError();
 }
 

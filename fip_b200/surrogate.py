@@ -5,8 +5,14 @@ Network (every convolution 3x3, BF16 operands, FP32 accumulation on the tcgen05 
 libfip_b200 kernels of include/fip_surrogate.h):
   input  6 features per cell (terrain, kSt, water level, qx, qy, wet mask), zero-padded to 64
   stem   conv 64 -> 64 + ReLU
-  8 residual blocks   a' = relu(a + conv(relu(conv(a))))          (16 convolutions)
-  head   conv 64 -> 3: (dz / 0.5 m, dqx / 1 m2/s, dqy / 1 m2/s) over the next 60 s
+  8 residual blocks   a' = relu(a + conv_d(relu(conv_d(a))))      (16 convolutions)
+  head   conv 64 -> 4: mean discharges through each cell's east and north faces over the next
+         60 s (Fx, Fy) and the changes of qx and qy; the depth changes by the discrete
+         continuity equation dh = -(60 / dx) (Fx - Fx_west + Fy - Fy_south), so the surrogate
+         moves water between neighbours and through the domain edge only (mass conserving)
+The 3x3 kernels of block k are dilated by d = 1, 2, 4, 8, 1, 2, 4, 8: the network sees 62 cells
+(186 m) around a cell, about as far as a flood front travels in 60 s; undilated it would see 18.
+Tensors carry a zero border of 8 pixels (FIP_SG_PAD) so that every dilated tap stays inside.
 The head starts at zero, so an untrained network is persistence (nothing changes); training
 learns the change. Cells held by boundary conditions are reset to their condition's values
 after every call (`pin`). AdamW on an FP32 master copy; the bf16 weights of the forward and of
@@ -25,9 +31,11 @@ import numpy as np
 from . import _lib
 
 C = 64
+PAD = 8
 TAP = 9 * C * C
 LAYER = TAP + C  # weights then biases of one layer
 N_LAYERS = 18    # stem, 8 x 2 block convolutions, head
+DIL = [1] + [d for d in (1, 2, 4, 8, 1, 2, 4, 8) for _ in range(2)] + [1]
 EPI_BIAS_RELU, EPI_BIAS_RES_RELU, EPI_HEAD, EPI_MASK, EPI_RES_MASK, EPI_PLAIN = range(6)
 OUT_Z, OUT_Q = 0.5, 1.0
 
@@ -104,9 +112,11 @@ class Surrogate:
         key = (N, H, W, train)
         if key not in self._bufs:
             torch = self.torch
-            shape = (N, H + 2, W + 2, C)
+            shape = (N, H + 2 * PAD, W + 2 * PAD, C)
             act = lambda: torch.zeros(shape, dtype=torch.bfloat16, device=self.dev)  # noqa: E731
-            b = {"x": act(), "pred": torch.zeros((N, H + 2, W + 2, 4), dtype=torch.float32, device=self.dev)}
+            b = {"x": act(),
+                 "pred": torch.zeros((N, H + 2 * PAD, W + 2 * PAD, 4), dtype=torch.float32, device=self.dev)}
+            b["e"] = torch.zeros((N, H, W), dtype=torch.float32, device=self.dev)
             if train:
                 b["a"] = [act() for _ in range(9)]
                 b["h"] = [act() for _ in range(8)]
@@ -122,8 +132,8 @@ class Surrogate:
         w = _ptr(self.wd if grad else self.wf, layer * TAP)
         bias = None if grad or epi in (EPI_MASK, EPI_RES_MASK, EPI_PLAIN) else _ptr(self.p, layer * LAYER + TAP)
         _lib.check(self.L.fip_sg_conv3x3(_ptr(src), w, bias, _ptr(res) if res is not None else None,
-                                         _ptr(mask) if mask is not None else None, _ptr(out), N, H, W, epi,
-                                         _ptr(self.err), _stream()))
+                                         _ptr(mask) if mask is not None else None, _ptr(out), N, H, W, DIL[layer],
+                                         epi, _ptr(self.err), _stream()))
 
     # ---- forward / backward ------------------------------------------------------------------
     def pack(self, h, qx, qy, terrain, kst, zref, no_value, N, H, W, train=False):
@@ -151,10 +161,11 @@ class Surrogate:
         A, Hb, G = b["a"], b["h"], b["g"]
         L, st, err = self.L, _stream(), _ptr(self.err)
         self.g.zero_()
-        n_pix = N * (H + 2) * (W + 2)
+        n_pix = N * (H + 2 * PAD) * (W + 2 * PAD)
 
         def wgrad(x, dy, layer):
-            _lib.check(L.fip_sg_conv3x3_wgrad(_ptr(x), _ptr(dy), _ptr(self.g, layer * LAYER), N, H, W, err, st))
+            _lib.check(L.fip_sg_conv3x3_wgrad(_ptr(x), _ptr(dy), _ptr(self.g, layer * LAYER), N, H, W, DIL[layer],
+                                              err, st))
             _lib.check(L.fip_sg_bias_grad(_ptr(dy), n_pix, _ptr(self.g, layer * LAYER + TAP), st))
 
         gout = G[0]
@@ -171,11 +182,13 @@ class Surrogate:
             g, spare = spare, g
         wgrad(b["x"], g, 0)
 
-    def loss(self, tgt, N, H, W) -> None:
-        """Adds the summed squared error to self.loss_acc and puts d(mse)/d(pred) into g[0]."""
+    def loss(self, tgt, N, H, W, dx: float = 3.0) -> None:
+        """Adds the summed squared error of (dh / 0.5 m, dqx, dqy) to self.loss_acc and puts
+        d(mse)/d(pred) into g[0]."""
         b = self._buffers(N, H, W, True)
         b["g"][0].zero_()
-        _lib.check(self.L.fip_sg_loss(_ptr(b["pred"]), _ptr(tgt), N, H, W, _ptr(b["g"][0]), _ptr(self.loss_acc), _stream()))
+        _lib.check(self.L.fip_sg_loss(_ptr(b["pred"]), _ptr(tgt), N, H, W, float(dx), _ptr(b["e"]), _ptr(b["g"][0]),
+                                      _ptr(self.loss_acc), _stream()))
 
     def update(self, lr=3e-4, betas=(0.9, 0.999), eps=1e-8, weight_decay=1e-4):
         self.steps += 1
@@ -193,9 +206,9 @@ class Surrogate:
         self.pack(h, qx, qy, state["terrain"], state["kst"], state["zref"], state["no_value"], N, H, W)
         pred = self.forward(N, H, W)
         dvol = self.torch.zeros(N, dtype=self.torch.float64, device=self.dev)
-        _lib.check(self.L.fip_sg_apply(_ptr(pred), N, H, W, _ptr(state["terrain"]), float(state["no_value"]), _ptr(h),
-                                       _ptr(qx), _ptr(qy), _ptr(dvol), _ptr(hmax) if hmax is not None else None,
-                                       _stream()))
+        _lib.check(self.L.fip_sg_apply(_ptr(pred), N, H, W, float(state.get("dx", 3.0)), _ptr(state["terrain"]),
+                                       float(state["no_value"]), _ptr(h), _ptr(qx), _ptr(qy), _ptr(dvol),
+                                       _ptr(hmax) if hmax is not None else None, _stream()))
         if pins is not None:
             _lib.check(self.L.fip_sg_pin(_ptr(pins["mask"]), _ptr(pins["h"]), _ptr(pins["qx"]), _ptr(pins["qy"]),
                                          h.numel(), _ptr(h), _ptr(qx), _ptr(qy), _stream()))
@@ -230,10 +243,10 @@ def bench_convs(N: int = 32, H: int = 512, W: int = 512, iters: int = 20, device
     res = {}
     runs = {
         "forward": lambda: L.fip_sg_conv3x3(_ptr(x), _ptr(net.wf, TAP), _ptr(net.p, LAYER + TAP), None, None, _ptr(y),
-                                            N, H, W, EPI_BIAS_RELU, err, st),
-        "dgrad": lambda: L.fip_sg_conv3x3(_ptr(x), _ptr(net.wd, TAP), None, None, _ptr(x), _ptr(y), N, H, W, EPI_MASK,
-                                          err, st),
-        "wgrad": lambda: L.fip_sg_conv3x3_wgrad(_ptr(x), _ptr(y), _ptr(dw), N, H, W, err, st),
+                                            N, H, W, 1, EPI_BIAS_RELU, err, st),
+        "dgrad": lambda: L.fip_sg_conv3x3(_ptr(x), _ptr(net.wd, TAP), None, None, _ptr(x), _ptr(y), N, H, W, 1,
+                                          EPI_MASK, err, st),
+        "wgrad": lambda: L.fip_sg_conv3x3_wgrad(_ptr(x), _ptr(y), _ptr(dw), N, H, W, 1, err, st),
     }
     for name, fn in runs.items():
         for _ in range(3):

@@ -109,7 +109,12 @@ def solver_trajectories(scenarios, n_calls: int, device=0):
 
 
 def train(net: Surrogate, batch: Batch, snaps, steps: int, bs: int = 32, lr: float = 1e-3, seed: int = 0,
-          log_every: int = 50):
+          log_every: int = 50, pushforward: float = 0.0):
+    """AdamW on (state at t, state at t + 60 s) pairs with a cosine learning rate. With
+    pushforward p > 0, after the first quarter of the steps a fraction p of the steps start from
+    the network's own 60-s prediction out of the state at t - 60 s (no gradient through that
+    call) and learn the change to the solver's state at t + 60 s, so that the network learns to
+    correct the errors it makes itself in closed-loop use."""
     torch = _torch()
     T = snaps["h"].shape[0] - 1
     B, H, W = batch.n, batch.H, batch.W
@@ -121,17 +126,26 @@ def train(net: Surrogate, batch: Batch, snaps, steps: int, bs: int = 32, lr: flo
     terr = torch.empty((bs, H, W), dtype=torch.float32, device=dev)
     kst = torch.empty_like(terr)
     zref = torch.empty(bs, dtype=torch.float32, device=dev)
+    pins = {k: torch.empty((bs, H, W), dtype=v.dtype, device=dev) for k, v in batch.pins.items()}
     log = []
     t0 = time.perf_counter()
     for it in range(steps):
-        ti = torch.from_numpy(rng.integers(0, T, bs)).to(dev)
+        push = pushforward > 0 and it >= steps // 4 and rng.random() < pushforward and T >= 2
+        ti_np = rng.integers(1 if push else 0, T, bs)
+        ti = torch.from_numpy(ti_np).to(dev)
         mi = torch.from_numpy(rng.integers(0, B, bs)).to(dev)
-        for k in ("h", "qx", "qy"):
-            cur[k].copy_(snaps[k][ti, mi])
-            nxt[k].copy_(snaps[k][ti + 1, mi])
         terr.copy_(batch.terrain[mi])
         kst.copy_(batch.kst[mi])
         zref.copy_(batch.zref[mi])
+        for k in ("h", "qx", "qy"):
+            cur[k].copy_(snaps[k][ti - 1 if push else ti, mi])
+            nxt[k].copy_(snaps[k][ti + 1, mi])
+        if push:  # the network's own state at t
+            for k, v in batch.pins.items():
+                pins[k].copy_(v[mi])
+            st = {"h": cur["h"], "qx": cur["qx"], "qy": cur["qy"], "terrain": terr, "kst": kst, "zref": zref,
+                  "no_value": batch.no_value}
+            net.advance(st, pins)
         net.target(cur, nxt, terr, batch.no_value, tgt)
         net.pack(cur["h"], cur["qx"], cur["qy"], terr, kst, zref, batch.no_value, bs, H, W, train=True)
         net.forward(bs, H, W, train=True)
@@ -155,6 +169,24 @@ def _iou(a, b, thr=0.05):
     wa, wb = a > thr, b > thr
     u = np.logical_or(wa, wb).sum()
     return float(np.logical_and(wa, wb).sum() / u) if u else 1.0
+
+
+def rollout_trace(net: Surrogate, batch: Batch, snaps, calls=(1, 2, 5, 10, 20, 40, 60)):
+    """Depth RMSE and water volume (surrogate / solver) of a closed-loop run at the given calls."""
+    torch = _torch()
+    T = snaps["h"].shape[0] - 1
+    st = {k: snaps[k][0].clone() for k in ("h", "qx", "qy")}
+    state = batch.state(st["h"], st["qx"], st["qy"])
+    out = []
+    for c in range(1, T + 1):
+        net.advance(state, batch.pins)
+        if c in calls:
+            ref = snaps["h"][c].cpu().numpy().astype(np.float64)
+            got = st["h"].cpu().numpy().astype(np.float64)
+            out.append({"call": c, "rmse_depth_m": float(np.sqrt(np.mean((got - ref) ** 2))),
+                        "volume_ratio": float(got.sum() / max(ref.sum(), 1e-9))})
+    torch.cuda.synchronize()
+    return out
 
 
 def evaluate_one_call(net: Surrogate, batch: Batch, snaps):
@@ -214,6 +246,7 @@ def main(argv=None, emit: bool = True):
     ap.add_argument("--steps", type=int, default=400, help="training steps")
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--pushforward", type=float, default=0.5)
     ap.add_argument("--eval-members", type=int, default=8)
     ap.add_argument("--screen-members", type=int, default=32)
     ap.add_argument("--screen-size", type=int, default=512)
@@ -231,7 +264,7 @@ def main(argv=None, emit: bool = True):
     res["train_data"] = {"pairs": a.members * n_calls, "solver_s": round(t_gen, 2)}
     # ---- training
     net = Surrogate(seed=0)
-    log, t_train = train(net, btr, snaps, a.steps, bs=a.batch, lr=a.lr)
+    log, t_train = train(net, btr, snaps, a.steps, bs=a.batch, lr=a.lr, pushforward=a.pushforward)
     res["train"] = {"loss_log": log, "seconds": round(t_train, 2), "steps": a.steps,
                     "ms_per_step": round(1e3 * t_train / max(a.steps, 1), 2)}
     del snaps
@@ -241,6 +274,7 @@ def main(argv=None, emit: bool = True):
     bev = Batch(ev)
     esn, ehmax, _ = solver_trajectories(ev, n_calls)
     res["eval_one_call"] = evaluate_one_call(net, bev, esn)
+    res["eval_trace"] = rollout_trace(net, bev, esn)
     st, hm, tripped, worst = rollout(net, bev, n_calls, esn["h"][0], esn["qx"][0], esn["qy"][0])
     ref_h = esn["h"][n_calls].cpu().numpy()
     got_h = st["h"].cpu().numpy()

