@@ -133,6 +133,15 @@ int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, doub
   return sg_cuda(fip::sg::edge_flux(qx, qy, N, H, W, flux, SG_S), "fip_sg_edge_flux");
 }
 
+int fip_sg_edges(float* h, const float* terrain, int N, int H, int W, int t_left, int t_right, int t_top, int t_bottom,
+                 float no_value, void* stream) {
+  if (!h || !terrain || N <= 0 || H < 3 || W < 3) return sg_fail(FIP_ERR_ARG, "fip_sg_edges: bad argument");
+  const int types[4] = {t_left, t_right, t_top, t_bottom};
+  for (int t : types)
+    if (t < 0 || t > 2) return sg_fail(FIP_ERR_ARG, "fip_sg_edges: side type must be 0 (none), 1 (close) or 2 (open)");
+  return sg_cuda(fip::sg::edge_cells(h, terrain, N, H, W, types, no_value, SG_S), "fip_sg_edges");
+}
+
 int fip_sg_pin(const unsigned char* mask, const float* h_val, const float* qx_val, const float* qy_val, long long total,
                float* h, float* qx, float* qy, void* stream) {
   if (!mask || !h_val || !qx_val || !qy_val || !h || !qx || !qy || total <= 0)

@@ -76,8 +76,9 @@ __global__ void target_kernel(const float* __restrict__ h0, const float* __restr
   tgt[3 * i + 2] = valid ? (qy1[i] - qy0[i]) * (1.f / kOutQ) : 0.f;
 }
 
-// loss = mean over interior cells and 3 outputs of the squared errors of (dh / kOutZ, dqx, dqy)
-// against the target. Pass 1: the loss and e[i] = d loss / d(dh / kOutZ) per cell.
+// loss = squared errors of (dh / kOutZ, dqx, dqy) against the target, summed over the cells (the
+// depth term over the inner cells [2, W-2] x [1, H-2] only) and divided by 3 N H W.
+// Pass 1: the loss and e[i] = d loss / d(dh / kOutZ) per cell.
 __global__ void loss_pass1_kernel(const float* __restrict__ pred, const float* __restrict__ tgt, int N, int H, int W,
                                   float c, float inv_count, float* __restrict__ e, double* __restrict__ loss) {
   __shared__ double red[256];
@@ -88,7 +89,11 @@ __global__ void loss_pass1_kernel(const float* __restrict__ pred, const float* _
     const int n = (int)(i / ((size_t)H * W));
     const int y = (int)((i / W) % H), x = (int)(i % W);
     const size_t p = ppix(n, y, x, H, W);
-    const float d0 = dh_of(pred, p, W + 2 * kPad, c) * (1.f / kOutZ) - tgt[3 * i + 0];
+    // only cells the continuity equation updates carry a depth error: the edge cells (and the
+    // second column, which a z condition on the left edge also sets) get their depths from the
+    // boundary conditions, and fitting them would push the discharges through their faces to 0
+    const bool inner = x >= 2 && x <= W - 2 && y >= 1 && y <= H - 2;
+    const float d0 = inner ? dh_of(pred, p, W + 2 * kPad, c) * (1.f / kOutZ) - tgt[3 * i + 0] : 0.f;
     const float d1 = pred[p * 4 + 2] - tgt[3 * i + 1];
     const float d2 = pred[p * 4 + 3] - tgt[3 * i + 2];
     acc = (double)d0 * d0 + (double)d1 * d1 + (double)d2 * d2;
@@ -192,14 +197,17 @@ __global__ void apply_kernel(const float* __restrict__ pred, int N, int H, int W
     if (terr[i] != no_value) {
       const size_t p = ppix(n, y, x, H, W);
       const float h0 = h[i];
-      const float h1 = fmaxf(0.f, h0 + dh_of(pred, p, W + 2 * kPad, c));
+      // continuity moves the depth of the inner cells; the edge cells follow the boundary
+      // conditions (fip_sg_edges, pins), as in the solver
+      const bool inner = x >= 2 && x <= W - 2 && y >= 1 && y <= H - 2;
+      const float h1 = inner ? fmaxf(0.f, h0 + dh_of(pred, p, W + 2 * kPad, c)) : h0;
       h[i] = h1;
       if (hmax) hmax[i] = fmaxf(hmax[i], h1);
       qx[i] += pred[p * 4 + 2] * kOutQ;
       qy[i] += pred[p * 4 + 3] * kOutQ;
       // volume of the cells only the continuity equation updates (a z condition on the left
       // edge also sets column 1): its change must match the discharge through the faces around
-      if (x >= 2 && x <= W - 2 && y >= 1 && y <= H - 2) dv = (double)h1 - (double)h0;
+      if (inner) dv = (double)h1 - (double)h0;
     }
   }
   if (threadIdx.x == 0) s_n0 = (int)(((size_t)blockIdx.x * blockDim.x) / img);
@@ -260,7 +268,39 @@ __global__ void pin_kernel(const unsigned char* __restrict__ mask, const float* 
   if (m & 4u) qy[i] = qyv[i];
 }
 
+// Edge cells by boundary type after a surrogate call, per side (left, right, top, bottom):
+// 0 none (the solver never writes the edge: keep), 1 close (depth of the inner neighbour,
+// src/bc_kernel_gen.cpp:112-116), 2 open (min(h_nb, max(0, z_nb - terrain)), :128-136).
+__global__ void edges_kernel(float* __restrict__ h, const float* __restrict__ terr, int N, int H, int W, int t_left,
+                             int t_right, int t_top, int t_bottom, float no_value) {
+  const int n = blockIdx.y;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  float* hn = h + (size_t)n * H * W;
+  const float* tn = terr + (size_t)n * H * W;
+  auto set = [&](int type, size_t e, size_t nb) {
+    if (type == 0 || tn[e] == no_value) return;
+    const float hb = hn[nb];
+    hn[e] = type == 1 ? hb : (hb > 0.f ? fminf(hb, fmaxf(0.f, hb + tn[nb] - tn[e])) : hn[e]);
+  };
+  if (k < H) {
+    set(t_left, (size_t)k * W, (size_t)k * W + 1);
+    set(t_right, (size_t)k * W + (W - 1), (size_t)k * W + (W - 2));
+  }
+  if (k < W) {
+    set(t_bottom, (size_t)k, (size_t)W + k);
+    set(t_top, (size_t)(H - 1) * W + k, (size_t)(H - 2) * W + k);
+  }
+}
+
 }  // namespace
+
+cudaError_t edge_cells(float* h, const float* terr, int N, int H, int W, const int* types, float no_value,
+                       cudaStream_t s) {
+  const int n = H > W ? H : W;
+  edges_kernel<<<dim3((n + 255) / 256, N), 256, 0, s>>>(h, terr, N, H, W, types[0], types[1], types[2], types[3],
+                                                       no_value);
+  return cudaGetLastError();
+}
 
 cudaError_t pin_cells(const unsigned char* mask, const float* hv, const float* qxv, const float* qyv, size_t total,
                       float* h, float* qx, float* qy, cudaStream_t s) {

@@ -209,10 +209,20 @@ class Surrogate:
         _lib.check(self.L.fip_sg_apply(_ptr(pred), N, H, W, float(state.get("dx", 3.0)), _ptr(state["terrain"]),
                                        float(state["no_value"]), _ptr(h), _ptr(qx), _ptr(qy), _ptr(dvol),
                                        _ptr(hmax) if hmax is not None else None, _stream()))
+        sides = state.get("sides")
+        if sides is not None:  # (left, right, top, bottom): 0 none, 1 close, 2 open
+            _lib.check(self.L.fip_sg_edges(_ptr(h), _ptr(state["terrain"]), N, H, W, *[int(t) for t in sides],
+                                           float(state["no_value"]), _stream()))
         if pins is not None:
             _lib.check(self.L.fip_sg_pin(_ptr(pins["mask"]), _ptr(pins["h"]), _ptr(pins["qx"]), _ptr(pins["qy"]),
                                          h.numel(), _ptr(h), _ptr(qx), _ptr(qy), _stream()))
         return dvol
+
+    def pin(self, state, pins):
+        """Cells held by boundary conditions get their condition's values."""
+        h = state["h"]
+        _lib.check(self.L.fip_sg_pin(_ptr(pins["mask"]), _ptr(pins["h"]), _ptr(pins["qx"]), _ptr(pins["qy"]),
+                                     h.numel(), _ptr(h), _ptr(state["qx"]), _ptr(state["qy"]), _stream()))
 
     def edge_flux(self, qx, qy):
         N, H, W = qx.shape

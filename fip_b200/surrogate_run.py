@@ -81,9 +81,12 @@ class Batch:
         self.no_value = -9999.0
         self.cells = self.n * self.H * self.W
 
+    # edge types of the generator's scenarios (left z is pinned; right open; top and bottom close)
+    SIDES = (0, 2, 1, 1)
+
     def state(self, h, qx, qy):
         return {"h": h, "qx": qx, "qy": qy, "terrain": self.terrain, "kst": self.kst, "zref": self.zref,
-                "no_value": self.no_value}
+                "no_value": self.no_value, "sides": self.SIDES}
 
 
 def solver_trajectories(scenarios, n_calls: int, device=0):
@@ -140,11 +143,12 @@ def train(net: Surrogate, batch: Batch, snaps, steps: int, bs: int = 32, lr: flo
         for k in ("h", "qx", "qy"):
             cur[k].copy_(snaps[k][ti - 1 if push else ti, mi])
             nxt[k].copy_(snaps[k][ti + 1, mi])
+        for k, v in batch.pins.items():
+            pins[k].copy_(v[mi])
+        st = {"h": cur["h"], "qx": cur["qx"], "qy": cur["qy"], "terrain": terr, "kst": kst, "zref": zref,
+              "no_value": batch.no_value, "sides": batch.SIDES}
+        net.pin(st, pins)  # the first snapshot precedes the iteration-0 boundary conditions
         if push:  # the network's own state at t
-            for k, v in batch.pins.items():
-                pins[k].copy_(v[mi])
-            st = {"h": cur["h"], "qx": cur["qx"], "qy": cur["qy"], "terrain": terr, "kst": kst, "zref": zref,
-                  "no_value": batch.no_value}
             net.advance(st, pins)
         net.target(cur, nxt, terr, batch.no_value, tgt)
         net.pack(cur["h"], cur["qx"], cur["qy"], terr, kst, zref, batch.no_value, bs, H, W, train=True)
@@ -177,6 +181,7 @@ def rollout_trace(net: Surrogate, batch: Batch, snaps, calls=(1, 2, 5, 10, 20, 4
     T = snaps["h"].shape[0] - 1
     st = {k: snaps[k][0].clone() for k in ("h", "qx", "qy")}
     state = batch.state(st["h"], st["qx"], st["qy"])
+    net.pin(state, batch.pins)
     out = []
     for c in range(1, T + 1):
         net.advance(state, batch.pins)
@@ -197,10 +202,12 @@ def evaluate_one_call(net: Surrogate, batch: Batch, snaps):
     n = 0
     for t in range(T):
         st = {k: snaps[k][t].clone() for k in ("h", "qx", "qy")}
-        net.advance(batch.state(st["h"], st["qx"], st["qy"]), batch.pins)
+        s0 = batch.state(st["h"], st["qx"], st["qy"])
+        net.pin(s0, batch.pins)
+        pers = st["h"].cpu().numpy()  # persistence = the untrained network: pinned input unchanged
+        net.advance(s0, batch.pins)
         ref = snaps["h"][t + 1].cpu().numpy()
         got = st["h"].cpu().numpy()
-        pers = snaps["h"][t].cpu().numpy()
         se_net += float(np.sum((got.astype(np.float64) - ref) ** 2))
         se_pers += float(np.sum((pers.astype(np.float64) - ref) ** 2))
         n += ref.size
@@ -216,11 +223,12 @@ def rollout(net: Surrogate, batch: Batch, n_calls: int, h0, qx0, qy0, residual_t
     torch = _torch()
     st = {"h": h0.clone(), "qx": qx0.clone(), "qy": qy0.clone()}
     state = batch.state(st["h"], st["qx"], st["qy"])
+    net.pin(state, batch.pins)  # the iteration-0 boundary conditions
     hmax = st["h"].clone()
     tripped = np.zeros(batch.n, bool)
     worst = np.zeros(batch.n)
     dx = 3.0
-    h_host = h0.cpu().numpy()
+    h_host = st["h"].cpu().numpy()
     vol = h_host[:, 1:-1, 2:-1].astype(np.float64).sum(axis=(1, 2))
     # floor of the reference volume: 1 cm of water over 1 % of the inner cells (a dry start
     # would otherwise make every relative residual infinite)

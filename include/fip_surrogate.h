@@ -46,7 +46,8 @@ int fip_sg_target(const float* h0, const float* qx0, const float* qy0, const flo
 /* The network output pred (f32 [N][H+16][W+16][4]) holds per cell the mean discharges through
  * the east and north faces over the 60-s call (Fx, Fy, m2/s) and the changes of qx and qy; the
  * depth change is dh = -(60 / dx) (Fx - Fx_west + Fy - Fy_south) (mass conserving).
- * *loss += sum of squared errors of (dh / 0.5, dqx, dqy) against tgt; grad (bf16
+ * *loss += sum of squared errors of (dh / 0.5, dqx, dqy) against tgt (dh over the inner cells
+ * [2, W-2] x [1, H-2], whose depth only continuity changes); grad (bf16
  * [N][H+16][W+16][64], channels 0..3) = d(mean squared error)/d(pred); scratch holds N*H*W
  * floats. grad must be zeroed first. */
 int fip_sg_loss(const float* pred, const float* tgt, int N, int H, int W, float dx, float* scratch, void* grad,
@@ -60,8 +61,8 @@ int fip_sg_adamw(float* p, const float* g, float* m, float* v, long long n, floa
 /* bf16 copies of n_layers layers of f32 parameters: wf [l][9][out][in] for the forward
  * convolution, wd [l][9][in][out] with reversed taps for the input gradient. */
 int fip_sg_cast_weights(const float* p, int n_layers, void* wf, void* wd, void* stream);
-/* One surrogate call: h = max(0, h + dh) with dh from the face discharges, qx += pred2,
- * qy += pred3 (no-data cells kept);
+/* One surrogate call: h = max(0, h + dh) on the inner cells [2, W-2] x [1, H-2] with dh from the
+ * face discharges (edge cells: fip_sg_edges), qx += pred2, qy += pred3 (no-data cells kept);
  * dvol[n] += change of the depth sum over the inner cells [2, W-2] x [1, H-2] of image n
  * (H * W >= 256); hmax (may be NULL) = max(hmax, new h). */
 int fip_sg_apply(const float* pred, int N, int H, int W, float dx, const float* terrain, float no_value, float* h,
@@ -70,6 +71,10 @@ int fip_sg_apply(const float* pred, int N, int H, int W, float dx, const float* 
  * (through qx[:, 1], qx[:, W-2], qy[0, :], qy[H-2, :]). */
 int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, void* stream);
 
+/* Edge cells after a surrogate call by the boundary type of each side: 0 none (kept), 1 close
+ * (depth of the inner neighbour), 2 open (min(h_nb, max(0, z_nb - terrain))). */
+int fip_sg_edges(float* h, const float* terrain, int N, int H, int W, int t_left, int t_right, int t_top, int t_bottom,
+                 float no_value, void* stream);
 /* Cells fixed by boundary conditions: mask bit 0 sets h, bit 1 qx, bit 2 qy to the given values. */
 int fip_sg_pin(const unsigned char* mask, const float* h_val, const float* qx_val, const float* qy_val, long long total,
                float* h, float* qx, float* qy, void* stream);

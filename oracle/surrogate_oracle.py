@@ -6,7 +6,8 @@ Same network as fip_b200/surrogate.py, on unpadded NHWC arrays:
   h_k = relu(conv_d(a_k, W_{2k+1}) + b_{2k+1}),  a_{k+1} = relu(conv_d(h_k, W_{2k+2}) + b_{2k+2} + a_k)
   pred = conv(a_8, W17)[..., :4] + b17[:4]      (Fx, Fy, dqx, dqy)
   dh = -(60 / dx) (Fx - Fx_west + Fy - Fy_south)  (faces outside the image carry nothing)
-  loss = mean over cells and the 3 outputs of the squared errors of (dh / 0.5, dqx, dqy)
+  loss = squared errors of (dh / 0.5, dqx, dqy) summed over the cells (dh over the inner cells
+         [2, W-2] x [1, H-2] only: the edge cells follow the boundary conditions) / (3 N H W)
 with the dilation d of layer l given by DIL (block k: 1, 2, 4, 8, 1, 2, 4, 8).
 Gradients by reverse-mode differentiation of the same expressions (conv_oracle supplies the
 convolution and its two adjoints).
@@ -56,6 +57,9 @@ def loss_and_grads(p, x, target, dx=3.0):
     count = target.size
     c = 60.0 / dx
     d0 = depth_change(pred, dx) / 0.5 - target[..., 0]
+    inner = np.zeros(d0.shape[1:], bool)
+    inner[1:-1, 2:-1] = True  # depth error on the cells only continuity updates
+    d0 = np.where(inner, d0, 0.0)
     d1 = pred[..., 2] - target[..., 1]
     d2 = pred[..., 3] - target[..., 2]
     loss = float((np.sum(d0 * d0) + np.sum(d1 * d1) + np.sum(d2 * d2)) / count)
