@@ -6,7 +6,7 @@ fip_ref_nomask with the wet/dry mask off, fip_ref_sync = nomask + synchronised C
 This script needs a GPU: it writes small seeded scenarios, runs those binaries on them and
 packs inputs, the stdout sampling CSV and every save_state dump into one .npz per case.
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out /tmp/golden      (then copy the .npz files here)
 
 Grid sizes avoid the reference's two halo-lane defects (W mod 28 in {2,3,5}, H mod 50 in {2,3}).
 The cudaMallocPitch row pitch of each W is recorded, since the reference's open boundary on the
@@ -157,7 +157,7 @@ def case_g3(work: str, out: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="directory for the .npz fixtures")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     with tempfile.TemporaryDirectory() as work:

@@ -1,7 +1,7 @@
 """GPU parity of the sm_100a solver, through the C ABI (fip_b200.Simulation -> libfip_b200.so).
 
 * against the reference binary's own dumps and sampling rows (tests/golden/*.npz), with the
-  north-star gates: |dz| <= 1e-4 m, |dq| <= 1e-4 m^2/s (plus a relative term for the reference's
+  accuracy gates: |dz| <= 1e-4 m, |dq| <= 1e-4 m^2/s (plus a relative term for the reference's
   pitch-scaled top/bottom outflow, whose depths reach hundreds of metres), identical wet sets and
   the same step count;
 * against the CPU oracle (FP32 and FP64 builds) on random wet states with every boundary type,
