@@ -278,14 +278,10 @@ def run_gpu(args, rank, world, local_rank):
 
     from fip_b200 import Simulation
 
+    from fip_b200 import replicas
+
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist = replicas.init("nccl")
     sc = make_workload(args, rank)
     W, H = sc.W, sc.H
     cells = W * H
@@ -309,16 +305,12 @@ def run_gpu(args, rank, world, local_rank):
     # ---- headline: every tile computed ----
     sim = Simulation(sc.yaml_path, device=local_rank, quiet=True, all_tiles=True)
     sim.step_timed(max(args.warmup, 3))  # warm-up (graph build, clocks, TLB)
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     torch.cuda.synchronize()
     with Clocks(local_rank) as clk:
         total_ms, stencil_ms, post_ms = sim.step_timed(args.steps)
     torch.cuda.synchronize()
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = replicas.max_over_ranks(dist, total_ms, device="cuda")
     value = world * cells * args.steps / (total_ms / 1e3)
 
     # ---- e2e through the C ABI with pinned host buffers ----
@@ -330,8 +322,7 @@ def run_gpu(args, rank, world, local_rank):
     for k in hbuf:  # warm the path once
         sim.set_field(k, hbuf[k])
     sim.step(inner)
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     t0 = time.perf_counter()
     for _ in range(reps):
         for k in ("h", "qx", "qy"):
@@ -340,10 +331,7 @@ def run_gpu(args, rank, world, local_rank):
         for k in ("h", "qx", "qy"):
             sim.field(k, out=hbuf[k])
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_s = float(te.item())
+    e2e_s = replicas.max_over_ranks(dist, e2e_s, device="cuda")
     e2e_value = world * cells * inner * reps / e2e_s
     sim.close()
 
@@ -386,9 +374,7 @@ def run_gpu(args, rank, world, local_rank):
                 "gpu_launches": 2 * args.steps, "roofline": roof, "clocks": clocks,
                 "cpu_baseline": base, "active_tiles": active, "ensemble": ens, "surrogate": sgm}
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
     return 0
 
 
