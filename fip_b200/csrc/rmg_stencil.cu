@@ -10,7 +10,7 @@
 //   * the domain is cut into tiles of 480 columns x 32 rows. A CTA has four consumer warps
 //     (each thread owns 4 adjacent columns, a warp 128 columns of which the 120 inner ones are
 //     stored) and one producer warp that streams rows of h/qx/qy/terrain/kSt into a ring of 6
-//     rows (7 without kSt) in shared memory with TMA (cp.async.bulk.tensor, no multicast).
+//     rows (7 without kSt) in shared memory with TMA (cp.async.bulk.tensor; each CTA loads its own rows).
 //     Consumers march north row by row over the staged rows r-1 .. r+2, exchange east/west
 //     neighbours with warp shuffles and do the arithmetic on FP32x2 pairs of columns;
 //   * work = the concatenation of the active tiles' rows (strip-major), split evenly over the
