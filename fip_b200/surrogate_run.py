@@ -14,7 +14,7 @@ Workloads:
     batched solver; the result is judged against the batched solver on every member (max-depth
     RMSE, flooded-extent IoU at 5 cm, wall time).
 
-    python -m fip_b200.surrogate_run [--members 32 --size 512 --hours 1 --steps 400 ...]
+    python -m fip_b200.surrogate_run [--members 64 --size 512 --hours 1 --steps 2400 --unroll 3 ...]
 
 prints one JSON object with the measurements.
 """
@@ -112,12 +112,12 @@ def solver_trajectories(scenarios, n_calls: int, device=0):
 
 
 def train(net: Surrogate, batch: Batch, snaps, steps: int, bs: int = 32, lr: float = 1e-3, seed: int = 0,
-          log_every: int = 50, pushforward: float = 0.0):
+          log_every: int = 50, pushforward: float = 0.0, unroll: int = 1):
     """AdamW on (state at t, state at t + 60 s) pairs with a cosine learning rate. With
     pushforward p > 0, after the first quarter of the steps a fraction p of the steps start from
-    the network's own 60-s prediction out of the state at t - 60 s (no gradient through that
-    call) and learn the change to the solver's state at t + 60 s, so that the network learns to
-    correct the errors it makes itself in closed-loop use."""
+    the network's own state after k calls (k drawn from 1..unroll, no gradient through them) out
+    of the solver's state at t - 60 k s, and learn the change to the solver's state at t + 60 s,
+    so that the network learns to correct the errors it makes itself in closed-loop use."""
     torch = _torch()
     T = snaps["h"].shape[0] - 1
     B, H, W = batch.n, batch.H, batch.W
@@ -134,21 +134,22 @@ def train(net: Surrogate, batch: Batch, snaps, steps: int, bs: int = 32, lr: flo
     t0 = time.perf_counter()
     for it in range(steps):
         push = pushforward > 0 and it >= steps // 4 and rng.random() < pushforward and T >= 2
-        ti_np = rng.integers(1 if push else 0, T, bs)
+        k_un = int(rng.integers(1, min(unroll, T - 1) + 1)) if push else 0
+        ti_np = rng.integers(k_un, T, bs)
         ti = torch.from_numpy(ti_np).to(dev)
         mi = torch.from_numpy(rng.integers(0, B, bs)).to(dev)
         terr.copy_(batch.terrain[mi])
         kst.copy_(batch.kst[mi])
         zref.copy_(batch.zref[mi])
         for k in ("h", "qx", "qy"):
-            cur[k].copy_(snaps[k][ti - 1 if push else ti, mi])
+            cur[k].copy_(snaps[k][ti - k_un, mi])
             nxt[k].copy_(snaps[k][ti + 1, mi])
         for k, v in batch.pins.items():
             pins[k].copy_(v[mi])
         st = {"h": cur["h"], "qx": cur["qx"], "qy": cur["qy"], "terrain": terr, "kst": kst, "zref": zref,
               "no_value": batch.no_value, "sides": batch.SIDES}
         net.pin(st, pins)  # the first snapshot precedes the iteration-0 boundary conditions
-        if push:  # the network's own state at t
+        for _ in range(k_un):  # the network's own state at t
             net.advance(st, pins)
         net.target(cur, nxt, terr, batch.no_value, tgt)
         net.pack(cur["h"], cur["qx"], cur["qy"], terr, kst, zref, batch.no_value, bs, H, W, train=True)
@@ -248,13 +249,14 @@ def rollout(net: Surrogate, batch: Batch, n_calls: int, h0, qx0, qy0, residual_t
 
 def main(argv=None, emit: bool = True):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--members", type=int, default=32, help="training trajectories")
+    ap.add_argument("--members", type=int, default=64, help="training trajectories")
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--hours", type=float, default=1.0, help="simulated length of each training trajectory")
-    ap.add_argument("--steps", type=int, default=400, help="training steps")
+    ap.add_argument("--steps", type=int, default=2400, help="training steps")
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr", type=float, default=5e-4)
     ap.add_argument("--pushforward", type=float, default=0.5)
+    ap.add_argument("--unroll", type=int, default=3, help="pushforward: up to this many own calls")
     ap.add_argument("--eval-members", type=int, default=8)
     ap.add_argument("--screen-members", type=int, default=32)
     ap.add_argument("--screen-size", type=int, default=512)
@@ -272,7 +274,7 @@ def main(argv=None, emit: bool = True):
     res["train_data"] = {"pairs": a.members * n_calls, "solver_s": round(t_gen, 2)}
     # ---- training
     net = Surrogate(seed=0)
-    log, t_train = train(net, btr, snaps, a.steps, bs=a.batch, lr=a.lr, pushforward=a.pushforward)
+    log, t_train = train(net, btr, snaps, a.steps, bs=a.batch, lr=a.lr, pushforward=a.pushforward, unroll=a.unroll)
     res["train"] = {"loss_log": log, "seconds": round(t_train, 2), "steps": a.steps,
                     "ms_per_step": round(1e3 * t_train / max(a.steps, 1), 2)}
     del snaps
