@@ -39,7 +39,8 @@ int fip_sg_conv3x3(const void* in, const void* w, const float* bias, const void*
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: this epilogue needs res");
   if ((epi == FIP_SG_EPI_MASK || epi == FIP_SG_EPI_RES_MASK) && !mask)
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: this epilogue needs mask");
-  if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(out)) & 15u)
+  if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(out) |
+       reinterpret_cast<uintptr_t>(res) | reinterpret_cast<uintptr_t>(mask)) & 15u)
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: tensors must be 16-byte aligned");
   if ((long long)N * (H + 2 * fip::sg::kPad) * (W + 2 * fip::sg::kPad) >= (1LL << 31))
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3: too many pixels");
@@ -56,6 +57,7 @@ int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H,
   if (!x || !dy || !dw || N <= 0 || H <= 0 || W <= 0) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: bad argument");
   if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(dy)) & 15u)
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: tensors must be 16-byte aligned");
+  if (dilation < 1 || dilation > fip::sg::kMaxDil) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: dilation must be 1..8");
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return sg_fail(FIP_ERR_ARG, "device ordinal");
@@ -69,7 +71,6 @@ int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H,
     }
     part = g_part[dev];
   }
-  if (dilation < 1 || dilation > fip::sg::kMaxDil) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: dilation must be 1..8");
   fip::sg::ConvShape s{N, H, W, dilation};
   return sg_cuda(fip::sg::conv3x3_wgrad(s, static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy),
                                         part, dw, dev_err, static_cast<cudaStream_t>(stream)),
@@ -82,6 +83,7 @@ int fip_sg_pack_input(const float* h, const float* qx, const float* qy, const fl
                       const float* zref, int N, int H, int W, float no_value, void* out, void* stream) {
   if (!h || !qx || !qy || !terrain || !kst || !zref || !out || N <= 0 || H <= 0 || W <= 0)
     return sg_fail(FIP_ERR_ARG, "fip_sg_pack_input: bad argument");
+  if (reinterpret_cast<uintptr_t>(out) & 15u) return sg_fail(FIP_ERR_ARG, "fip_sg_pack_input: out must be 16-byte aligned");
   return sg_cuda(fip::sg::pack_input(h, qx, qy, terrain, kst, zref, N, H, W, no_value, static_cast<__nv_bfloat16*>(out),
                                      SG_S),
                  "fip_sg_pack_input");
@@ -99,6 +101,7 @@ int fip_sg_loss(const float* pred, const float* tgt, int N, int H, int W, float 
                 double* loss, void* stream) {
   if (!pred || !tgt || !grad || !loss || !scratch || N <= 0 || H <= 0 || W <= 0 || !(dx > 0.f))
     return sg_fail(FIP_ERR_ARG, "fip_sg_loss: bad argument");
+  if (reinterpret_cast<uintptr_t>(grad) & 15u) return sg_fail(FIP_ERR_ARG, "fip_sg_loss: grad must be 16-byte aligned");
   return sg_cuda(fip::sg::loss_and_grad(pred, tgt, N, H, W, dx, scratch, static_cast<__nv_bfloat16*>(grad), loss, SG_S),
                  "fip_sg_loss");
 }

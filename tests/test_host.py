@@ -91,3 +91,20 @@ def test_boundary_program_compiles_for_sm100a(tmp_path):
     sc = synth.scenario1(str(tmp_path), W=64, H=48, seed=2, duration=600.0, name="p")
     src = bc_program(sc.yaml_path, 128, compile=True)
     assert "fip_post" in src and "fip_interp_block" in src and "fip_sum_depths" in src
+
+
+def test_surrogate_entry_points_reject_bad_arguments():
+    """Argument checks of include/fip_surrogate.h run on the host before any launch."""
+    L = _lib.lib()
+    vp = ctypes.c_void_p
+    assert L.fip_sg_conv3x3(None, None, None, None, None, None, 1, 8, 8, 1, 0, None, None) == _lib.FIP_ERR_ARG
+    odd = vp(0x1008)  # not 16-byte aligned (never dereferenced: rejected first)
+    al = vp(0x2000)
+    assert L.fip_sg_conv3x3(al, al, None, odd, None, al, 1, 8, 8, 1, 1, None, None) == _lib.FIP_ERR_ARG
+    assert L.fip_sg_conv3x3(al, al, None, None, None, al, 1, 8, 8, 9, 0, None, None) == _lib.FIP_ERR_ARG  # dilation
+    assert L.fip_sg_conv3x3(al, al, None, None, None, al, 1, 8, 8, 1, 7, None, None) == _lib.FIP_ERR_ARG  # epilogue
+    assert L.fip_sg_conv3x3(al, al, None, None, None, al, 1, 8, 8, 1, 1, None, None) == _lib.FIP_ERR_ARG  # needs res
+    assert L.fip_sg_conv3x3_wgrad(al, al, al, 1, 8, 8, 0, None, None) == _lib.FIP_ERR_ARG
+    assert L.fip_sg_edges(al, al, 1, 8, 8, 0, 3, 1, 1, ctypes.c_float(-1.0), None) == _lib.FIP_ERR_ARG
+    assert L.fip_sg_adamw(al, al, al, al, 10, ctypes.c_float(1e-3), ctypes.c_float(0.9), ctypes.c_float(0.999),
+                          ctypes.c_float(1e-8), ctypes.c_float(0.0), 0, None) == _lib.FIP_ERR_ARG  # step >= 1
