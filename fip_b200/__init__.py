@@ -113,6 +113,10 @@ class Simulation:
                                          os.fspath(png_path).encode() if png_path else None))
         return img
 
+    def inject_wait_timeout(self) -> None:
+        """Test hook: the next step's bounded device waits run out (FIP_ERR_DEVICE_TIMEOUT)."""
+        _lib.check(_lib.lib().fip_inject_wait_timeout(self._h))
+
     # -- exact resume ----------------------------------------------------------------------
     def checkpoint(self, path: str) -> None:
         """Writes both ping-pong buffers, hmax and the step state; see restore()."""

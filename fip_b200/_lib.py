@@ -34,7 +34,7 @@ EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_ru
            "fip_ensemble_destroy", "fip_checkpoint", "fip_restore", "fip_render", "fip_ensemble_render",
            "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad", "fip_ensemble_gather", "fip_sg_pack_input", "fip_sg_target",
            "fip_sg_loss", "fip_sg_bias_grad", "fip_sg_adamw", "fip_sg_cast_weights", "fip_sg_apply",
-           "fip_sg_edge_flux", "fip_sg_pin", "fip_sg_edges")
+           "fip_sg_edge_flux", "fip_sg_pin", "fip_sg_edges", "fip_inject_wait_timeout")
 
 
 class FipOptions(ctypes.Structure):
@@ -134,6 +134,8 @@ def lib():
                      "fip_sg_target", "fip_sg_loss", "fip_sg_bias_grad", "fip_sg_adamw", "fip_sg_cast_weights",
                      "fip_sg_apply", "fip_sg_edge_flux"):
             getattr(L, name).restype = ctypes.c_int
+        L.fip_inject_wait_timeout.argtypes = [vp]
+        L.fip_inject_wait_timeout.restype = ctypes.c_int
         L.fip_checkpoint.argtypes = [vp, ctypes.c_char_p]
         L.fip_restore.argtypes = [vp, ctypes.c_char_p]
         L.fip_checkpoint.restype = ctypes.c_int

@@ -54,7 +54,7 @@ struct FipCtl {
   int force_all;        // plan every tile as active (no dry-tile skipping)
   unsigned int cfl_bits[2];  // float bits of the running CFL minimum, by iteration parity
   unsigned int post_done;    // last-block-done counter of the post kernel
-  int pad_;
+  int inject;                // test hook: CTA 0 of the next stencil leaves its first row unstaged once
 };
 
 #define FIP_POST_MODE_STEP 0   // after a step: BCs at duration+dt, plan, advance the control block

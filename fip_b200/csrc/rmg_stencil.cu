@@ -361,6 +361,13 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       uint32_t seq = 0;
       bool ok = true;
       int s, ra, rb, m = 0;
+      // test hook (fip_inject_wait_timeout): the first row is never staged, so this CTA's waits
+      // for it run out and report FIP_DEVERR_* instead of hanging
+      bool skip_first = false;
+      if (blockIdx.x == 0 && ctl->inject) {
+        skip_first = true;
+        ctl->inject = 0;
+      }
       while (ok && (ENS ? next_run_ens(w, list, s_prefix, a.n_chunks, TR, a.members, s_tbase, a.n_members, &m, &s,
                                        &ra, &rb)
                         : next_run(w, list, s_prefix, a.n_chunks, a.n_ty, a.H, &s, &ra, &rb))) {
@@ -374,6 +381,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
             ok = false;
             break;
           }
+          if (skip_first && seq == 0) continue;
           unsigned char* dst = ring + slot * kSlotBytes;
           mbar_arrive_expect_tx(&full_bar[slot], kSlotBytes);
           const int y = y0 + j;
@@ -391,6 +399,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       const uint32_t n_in_flight = seq < (uint32_t)kNSlot ? seq : (uint32_t)kNSlot;
       for (uint32_t i = 0; i < n_in_flight; ++i) {
         const uint32_t q = seq - 1 - i;
+        if (skip_first && q == 0) continue;  // never issued
         if (!mbar_wait(&full_bar[q % kNSlot], (q / kNSlot) & 1u)) {
           record_error(ctl, FIP_DEVERR_WAIT_DRAIN);
           break;

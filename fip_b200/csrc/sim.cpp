@@ -800,6 +800,19 @@ int fip_set_field(fip_handle* h, int field, const float* src) {
   });
 }
 
+int fip_inject_wait_timeout(fip_handle* h) {
+  if (!h) return fail(FIP_ERR_ARG, "null handle");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    h->h_ctl->inject = 1;
+    ck(cudaMemcpyAsync(&h->d_ctl->inject, &h->h_ctl->inject, sizeof(int), cudaMemcpyHostToDevice, h->stream),
+       "fip_inject_wait_timeout");
+    ck(cudaStreamSynchronize(h->stream), "fip_inject_wait_timeout");
+    h->h_ctl->inject = 0;  // the device copy is cleared by the stencil that takes it
+    return FIP_OK;
+  });
+}
+
 int fip_time(fip_handle* h, double* duration, float* dt, int* iteration) {
   if (!h) return fail(FIP_ERR_ARG, "null handle");
   if (duration) *duration = h->h_ctl->duration;

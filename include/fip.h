@@ -144,6 +144,12 @@ int fip_restore(fip_handle* h, const char* path);
 #define FIP_RENDER_HMAX 2
 int fip_render(fip_handle* h, int what, float vmax, unsigned char* rgba_or_null, const char* png_path_or_null);
 
+/* Test hook of the failure detection (no counterpart in the reference): the next step's stencil
+ * leaves the first row of one CTA unstaged, so that CTA's bounded shared-memory waits run out
+ * (2 s) and the step returns FIP_ERR_DEVICE_TIMEOUT; the CUDA context stays usable, the handle
+ * does not (destroy it). */
+int fip_inject_wait_timeout(fip_handle* h);
+
 /* Frees every device and host resource of the handle (the reference leaves this to
  * cudaDeviceReset at exit, src/main.cpp:256). */
 void fip_destroy(fip_handle* h);
