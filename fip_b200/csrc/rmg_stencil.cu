@@ -69,7 +69,7 @@ struct StepArgs {
   // ensembles only: member table, per-member control, member count, tile rows
   const FipEnsMember* members;
   FipEnsCtl* mctl;
-  int n_members, tile_rows;
+  int n_members;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -118,6 +118,14 @@ __device__ __forceinline__ void tma_row(void* dst, const CUtensorMap* tm, int x,
       : "memory");
 }
 __device__ __forceinline__ void record_error(FipCtl* ctl, int code) { atomicCAS(&ctl->error, 0, code); }
+// Shared-memory values read where they are used: a volatile load is neither hoisted out of the
+// row loop nor merged with an earlier one, so the value holds no register between its uses.
+__device__ __forceinline__ int lds_at_use(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+__device__ __forceinline__ float ldsf_at_use(const float* p) { return *reinterpret_cast<const volatile float*>(p); }
+__device__ __forceinline__ float2 lds2_at_use(const float* p) {
+  const volatile float2* q = reinterpret_cast<const volatile float2*>(p);
+  return make_float2(q->x, q->y);
+}
 
 // FP32x2 arithmetic (sm_100 packed add/mul/fma): a thread owns 4 adjacent columns and applies
 // the same operation to all of them, so columns (0,1) and (2,3) go through one instruction each.
@@ -275,9 +283,10 @@ __device__ __forceinline__ bool next_run_ens(Walk& w, const int* list, const int
   return false;
 }
 
-// KW consumer warps per CTA (tiles of 120 * KW columns); ENS: the grid is a packed ensemble
-// (member table in the arguments, per-member dt, rows, sizes and CFL slots).
-template <bool KVAR, bool ENS, int KW>
+// KW consumer warps per CTA (tiles of 120 * KW columns, TRT rows); ENS: the grid is a packed
+// ensemble (member table in the arguments, per-member dt, rows, sizes and CFL slots). The tile
+// height is a template argument so that the row-to-tile arithmetic compiles to shifts and masks.
+template <bool KVAR, bool ENS, int KW, int TRT>
 __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
     rmg_step_kernel(const __grid_constant__ CUtensorMap tm_h0, const __grid_constant__ CUtensorMap tm_h1,
                     const __grid_constant__ CUtensorMap tm_qx0, const __grid_constant__ CUtensorMap tm_qx1,
@@ -300,6 +309,12 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
   __shared__ int s_prefix[kMaxChunks + 1];
   __shared__ int s_hdr[6];
   __shared__ int s_tbase[ENS ? FIP_ENS_MAX_MEMBERS + 1 : 1];
+  // ensemble: the current member's H, row offset, tile-flag base, tile rows, no_value, dx and
+  // index per consumer warp, read at their few uses so that they hold no registers through the
+  // row loop
+  __shared__ int s_msc[ENS ? KW : 1][7];
+  // ensemble: broadcast operands of the member's packed arithmetic (dt / dx dependent), the same way
+  __shared__ __align__(16) float s_mcf[ENS ? KW : 1][12];
 
   unsigned char* ring = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
   FipCtl* ctl = a.ctl;
@@ -344,7 +359,8 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
   const float dt = __int_as_float(s_hdr[3]);
   const bool fold = s_hdr[4] != 0;
   const int* list = a.list[it & 1];
-  const int TR = ENS ? a.tile_rows : FIP_TILE_ROWS;
+  constexpr int TR = TRT;
+  static_assert(TR == 16 || TR == 32 || TR == 64, "tile rows");
   const long long total = (long long)s_prefix[a.n_chunks] * TR;
   const long long G = gridDim.x;
   Walk walk0;
@@ -464,6 +480,23 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       nv = M.no_value;
       dtm = a.mctl[m].dt;
       set_scalars();
+      if (lane == 0) {
+        s_msc[warp][0] = H;
+        s_msc[warp][1] = row0;
+        s_msc[warp][2] = tbase;
+        s_msc[warp][3] = nty;
+        s_msc[warp][4] = __float_as_int(nv);
+        s_msc[warp][5] = __float_as_int(dx);
+        s_msc[warp][6] = m;
+        s_mcf[warp][0] = s_mcf[warp][1] = dt_inv;
+        s_mcf[warp][2] = s_mcf[warp][3] = dx;
+        s_mcf[warp][4] = s_mcf[warp][5] = dx_inv;
+        s_mcf[warp][6] = s_mcf[warp][7] = dtm;
+        s_mcf[warp][8] = s_mcf[warp][9] = -dtdx;
+        s_mcf[warp][10] = fric_u;
+        s_mcf[warp][11] = dtg;
+      }
+      __syncwarp();
     }
     const int c = s * TC - 4 + 120 * warp + 4 * lane;  // global column of k = 0
     // 4-bit column masks of the cell sets the reference's kernel writes (src/kernels.cu:383-406)
@@ -583,9 +616,9 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
           float kk[4] = {vk.x, vk.y, vk.z, vk.w};
           vmul(kk, kk, kk);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) fric[k] = dtg / kk[k];
+          for (int k = 0; k < 4; ++k) fric[k] = (ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg) / kk[k];
         } else {
-          fric[0] = fric[1] = fric[2] = fric[3] = fric_u;
+          fric[0] = fric[1] = fric[2] = fric[3] = ENS ? ldsf_at_use(&s_mcf[warp][10]) : fric_u;
         }
       }
       const float hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
@@ -604,8 +637,8 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
         ux1[k] = qx1[k] / fmaxf(fmaxf(kDH, h1[k]), k < 3 ? h1[k + 1] : hE1);
         uy1[k] = qy1[k] / fmaxf(fmaxf(kDH, h1[k]), h2r[k]);
       }
-      vmul(lim1, h1, c_dti);
-      vmul(lim1, lim1, c_dx);
+      vmul(lim1, h1, ENS ? lds2_at_use(&s_mcf[warp][0]) : c_dti);
+      vmul(lim1, lim1, ENS ? lds2_at_use(&s_mcf[warp][2]) : c_dx);
       vmul(lim1, lim1, c_q);
       const float ux1W = __shfl_up_sync(0xffffffffu, ux1[3], 1);
       const float uy1E = __shfl_down_sync(0xffffffffu, uy1[0], 1);
@@ -641,7 +674,8 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       const float fyW = __shfl_up_sync(0xffffffffu, fy[3], 1);
       const float fxE = __shfl_down_sync(0xffffffffu, fx[0], 1);
 
-      const bool hold_y = (r == 0 || r == H - 2);
+      const int Hr = ENS ? lds_at_use(&s_msc[warp][0]) : H;
+      const bool hold_y = (r == 0 || r == Hr - 2);
       // face depths and the mean cross discharges of the friction factor (:83-92, :110-119)
       float ax0[4], ax1[4], ay0[4], ay1[4], uyx[4], uxy[4];
 #pragma unroll
@@ -718,8 +752,8 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
         for (int k = 0; k < 4; ++k) u[k] = s0[k] - (k < 3 ? s0[k + 1] : sE0);  // -s_east + s_i
         vmul(t, ax0, c_g);
         vmul(t, t, u);
-        vfma(dsum, t, c_dxi, dsum);             // + dhg
-        vfma(dsum, c_dt, dsum, qx0);            // qx + dt * (...)
+        vfma(dsum, t, ENS ? lds2_at_use(&s_mcf[warp][4]) : c_dxi, dsum);  // + dhg
+        vfma(dsum, ENS ? lds2_at_use(&s_mcf[warp][6]) : c_dt, dsum, qx0);  // qx + dt * (...)
         vadd(t, c_one, rx);
 #pragma unroll
         for (int k = 0; k < 4; ++k) qx2[k] = dsum[k] / t[k];
@@ -742,8 +776,8 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
         vsub(u, s0, s1);
         vmul(t, ay0, c_g);
         vmul(t, t, u);
-        vfma(dsum, t, c_dxi, dsum);             // + dhg
-        vfma(dsum, c_dt, dsum, qy0);            // qy + dt * (...)
+        vfma(dsum, t, ENS ? lds2_at_use(&s_mcf[warp][4]) : c_dxi, dsum);  // + dhg
+        vfma(dsum, ENS ? lds2_at_use(&s_mcf[warp][6]) : c_dt, dsum, qy0);  // qy + dt * (...)
         vadd(t, c_one, ry);
 #pragma unroll
         for (int k = 0; k < 4; ++k) qy2[k] = dsum[k] / t[k];
@@ -760,18 +794,20 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       {
         const bool store_row = r >= ra;  // the extra row below a run only feeds qy2S
         int validm = 0;
+        const float nvr = ENS ? __int_as_float(lds_at_use(&s_msc[warp][4])) : nv;
+        const int Hs = ENS ? lds_at_use(&s_msc[warp][0]) : H;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) validm |= (s0[k] != nv) << k;
-        const int mH = (store_row && r >= 1 && r <= H - 2) ? (colHm & validm) : 0;
-        const int mQX = (store_row && r >= 2 && r <= H - 3) ? (colQXm & validm) : 0;
-        const int mQY = (store_row && r >= 1 && r <= H - 3) ? (colQYm & validm) : 0;
+        for (int k = 0; k < 4; ++k) validm |= (s0[k] != nvr) << k;
+        const int mH = (store_row && r >= 1 && r <= Hs - 2) ? (colHm & validm) : 0;
+        const int mQX = (store_row && r >= 2 && r <= Hs - 3) ? (colQXm & validm) : 0;
+        const int mQY = (store_row && r >= 1 && r <= Hs - 3) ? (colQYm & validm) : 0;
         // continuity (:381): h - dt * dx_inv * ((qx_i - qx_W) + (qy_i - qy_S))
         float h2[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) t[k] = qx2[k] - (k > 0 ? qx2[k - 1] : qx2W);
         vsub(u, qy2, qy2S);
         vadd(t, t, u);
-        vfma(h2, c_ndtdx, t, h0);
+        vfma(h2, ENS ? lds2_at_use(&s_mcf[warp][8]) : c_ndtdx, t, h0);
         // CFL of wet stored cells (:392-396): dx / (sqrt(G h') + max |u|), velocities of the old state
         vmul(t, c_g, h2);
 #pragma unroll
@@ -788,7 +824,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
           den_max = fmaxf(den_max, (wk && h2[k] > kEPS) ? t[k] : 0.0f);
           nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & 0x7fffffffu;
         }
-        const size_t row_off = (size_t)(r + row0) * (size_t)pitch + (size_t)c;
+        const size_t row_off = (size_t)(r + (ENS ? lds_at_use(&s_msc[warp][1]) : 0)) * (size_t)pitch + (size_t)c;
         if (mH == 15) {
           *reinterpret_cast<float4*>(h_out + row_off) = make_float4(h2[0], h2[1], h2[2], h2[3]);
         } else {
@@ -829,7 +865,10 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
         if (store_row && ((r + 1) % TR == 0 || r + 1 == rb)) {
           // halo lanes hold the neighbouring strips' cells; columns beyond W only occur in the last
           // strip, whose tiles are always computed anyway
-          if (__any_sync(0xffffffffu, out_lane && nzacc != 0u) && lane == 0) nzs[tbase + s * nty + r / TR] = 1;
+          if (__any_sync(0xffffffffu, out_lane && nzacc != 0u) && lane == 0) {
+            const int tb = ENS ? lds_at_use(&s_msc[warp][2]) : 0, nt = ENS ? lds_at_use(&s_msc[warp][3]) : nty;
+            nzs[tb + s * nt + r / TR] = 1;
+          }
           nzacc = 0u;
         }
       }
@@ -870,8 +909,8 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) dm = fmaxf(dm, __shfl_xor_sync(0xffffffffu, dm, off));
       if (lane == 0 && dm > 0.0f) {
-        const float cfl = fminf(1.0f, dx / dm);
-        if (cfl < 1.0f) atomicMin(&a.mctl[m].cfl_bits[it & 1], __float_as_uint(cfl));
+        const float cfl = fminf(1.0f, __int_as_float(lds_at_use(&s_msc[warp][5])) / dm);
+        if (cfl < 1.0f) atomicMin(&a.mctl[lds_at_use(&s_msc[warp][6])].cfl_bits[it & 1], __float_as_uint(cfl));
       }
       den_max = 0.0f;
     }
@@ -1041,7 +1080,7 @@ int rmg_step_grid(int device) {
   return kMinCtas * sms;
 }
 
-template <bool KVAR, bool ENS, int KW>
+template <bool KVAR, bool ENS, int KW, int TRT>
 static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t stream) {
   constexpr int NF = KVAR ? 5 : 4;
   constexpr int kNSlot = KW == 4 ? (KVAR ? kNSlotKvar : kNSlotUniform) : (KVAR ? kNSlotKvar2 : kNSlotUniform2);
@@ -1049,7 +1088,7 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
   static bool configured = false;
   if (!configured) {
     cudaError_t e =
-        cudaFuncSetAttribute(rmg_step_kernel<KVAR, ENS, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(rmg_step_kernel<KVAR, ENS, KW, TRT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
@@ -1077,20 +1116,29 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
   a.members = st.members;
   a.mctl = st.mctl;
   a.n_members = st.n_members;
-  a.tile_rows = st.tile_rows;
-  rmg_step_kernel<KVAR, ENS, KW><<<grid, (KW + 1) * 32, smem, stream>>>(
+  rmg_step_kernel<KVAR, ENS, KW, TRT><<<grid, (KW + 1) * 32, smem, stream>>>(
       st.tm_h[0], st.tm_h[1], st.tm_qx[0], st.tm_qx[1], st.tm_qy[0], st.tm_qy[1], st.tm_sohle, st.tm_kst, a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t stream) {
   if (st.n_chunks > kMaxChunks) return cudaErrorInvalidValue;
-  if (!st.members) return st.kst ? launch_step_t<true, false, 4>(st, grid, stream) : launch_step_t<false, false, 4>(st, grid, stream);
-  if (st.n_members > FIP_ENS_MAX_MEMBERS || st.tile_rows < 4) return cudaErrorInvalidValue;
-  if (st.kw == 4)
-    return st.kst ? launch_step_t<true, true, 4>(st, grid, stream) : launch_step_t<false, true, 4>(st, grid, stream);
-  if (st.kw == 2)
-    return st.kst ? launch_step_t<true, true, 2>(st, grid, stream) : launch_step_t<false, true, 2>(st, grid, stream);
+  constexpr int T = FIP_TILE_ROWS;
+  if (!st.members)
+    return st.kst ? launch_step_t<true, false, 4, T>(st, grid, stream) : launch_step_t<false, false, 4, T>(st, grid, stream);
+  if (st.n_members > FIP_ENS_MAX_MEMBERS) return cudaErrorInvalidValue;
+  // ensemble tile shapes: 2 or 4 consumer warps, 16, 32 or 64 rows
+#define FIP_ENS_LAUNCH(KW_, TR_)                                                                   \
+  if (st.kw == KW_ && st.tile_rows == TR_)                                                         \
+    return st.kst ? launch_step_t<true, true, KW_, TR_>(st, grid, stream)                          \
+                  : launch_step_t<false, true, KW_, TR_>(st, grid, stream);
+  FIP_ENS_LAUNCH(4, 32)
+  FIP_ENS_LAUNCH(4, 16)
+  FIP_ENS_LAUNCH(4, 64)
+  FIP_ENS_LAUNCH(2, 32)
+  FIP_ENS_LAUNCH(2, 16)
+  FIP_ENS_LAUNCH(2, 64)
+#undef FIP_ENS_LAUNCH
   return cudaErrorInvalidValue;
 }
 
