@@ -29,6 +29,7 @@
 #include "drv.h"
 #include "fip_ctl.h"
 #include "rmg_stencil.h"
+#include "smem_attr.h"
 
 namespace fip {
 
@@ -1085,13 +1086,9 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
   constexpr int NF = KVAR ? 5 : 4;
   constexpr int kNSlot = KW == 4 ? (KVAR ? kNSlotKvar : kNSlotUniform) : (KVAR ? kNSlotKvar2 : kNSlotUniform2);
   const int smem = kNSlot * NF * KW * 128 * 4 + 1024;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e =
-        cudaFuncSetAttribute(rmg_step_kernel<KVAR, ENS, KW, TRT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  static std::atomic<uint64_t> configured{0};
+  const cudaError_t e = ensure_dynamic_smem(rmg_step_kernel<KVAR, ENS, KW, TRT>, smem, configured);
+  if (e != cudaSuccess) return e;
   StepArgs a;
   for (int b = 0; b < 2; ++b) {
     a.h[b] = st.h[b];

@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include "drv.h"
+#include "smem_attr.h"
 #include "surrogate.h"
 
 namespace fip {
@@ -546,12 +547,9 @@ cudaError_t conv3x3(const ConvShape& s, const __nv_bfloat16* in, const __nv_bflo
   const int grid = std::min(conv_grid(), a.n_tiles);
 #define FIP_SG_LAUNCH(E)                                                                                  \
   case E: {                                                                                                \
-    static bool cfg = false;                                                                               \
-    if (!cfg) {                                                                                            \
-      cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); \
-      if (e != cudaSuccess) return e;                                                                      \
-      cfg = true;                                                                                          \
-    }                                                                                                      \
+    static std::atomic<uint64_t> cfg{0};                                                                   \
+    const cudaError_t e = ensure_dynamic_smem(conv3x3_kernel<E>, smem, cfg);                              \
+    if (e != cudaSuccess) return e;                                                                        \
     conv3x3_kernel<E><<<grid, kThreads, smem, stream>>>(tm_a, tm_w, a);                                    \
     break;                                                                                                 \
   }
@@ -586,12 +584,9 @@ cudaError_t conv3x3_wgrad(const ConvShape& s, const __nv_bfloat16* x, const __nv
   a.n_chunks = (n_pix + kWgChunk - 1) / kWgChunk;
   a.err = err;
   const int smem = kWgStages * kWgStageBytes + 1024;
-  static bool cfg = false;
-  if (!cfg) {
-    cudaError_t e = cudaFuncSetAttribute(conv3x3_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    cfg = true;
-  }
+  static std::atomic<uint64_t> cfg{0};
+  const cudaError_t e = ensure_dynamic_smem(conv3x3_wgrad_kernel, smem, cfg);
+  if (e != cudaSuccess) return e;
   const int grid = conv_grid();
   conv3x3_wgrad_kernel<<<grid, kThreads, smem, stream>>>(tm_x, tm_dy, a);
   wgrad_reduce_kernel<<<(9 * C * C + 255) / 256, 256, 0, stream>>>(part, grid, dw);
