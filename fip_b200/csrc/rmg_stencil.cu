@@ -1015,6 +1015,15 @@ __global__ void volume_partial_kernel(const float* __restrict__ h, int W, int H,
   if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
 }
 
+__global__ void flag_negative_kernel(const float* __restrict__ h, int W, int H, int pitch, int* flag) {
+  bool neg = false;
+  for (int r = blockIdx.x; r < H; r += gridDim.x) {
+    const float* row = h + (size_t)r * pitch;
+    for (int c = threadIdx.x; c < W; c += blockDim.x) neg |= row[c] < 0.f;
+  }
+  if (__syncthreads_or(neg) && threadIdx.x == 0) *flag = 1;
+}
+
 __global__ void volume_final_kernel(const double* partials, int n, double* out) {
   __shared__ double red[kVolThreads];
   double acc = 0.0;
@@ -1179,6 +1188,12 @@ int volume_partials(const StencilState&) { return kVolBlocks; }
 cudaError_t launch_volume(const StencilState& st, int parity, double* partials, double* out, cudaStream_t stream) {
   volume_partial_kernel<<<kVolBlocks, kVolThreads, 0, stream>>>(st.h[parity], st.W, st.H, st.pitch, partials);
   volume_final_kernel<<<1, kVolThreads, 0, stream>>>(partials, kVolBlocks, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_flag_negative(const float* h, int W, int H, int pitch, int* flag, cudaStream_t stream) {
+  if (W <= 0 || H <= 0) return cudaSuccess;
+  flag_negative_kernel<<<std::min(H, kVolBlocks), kVolThreads, 0, stream>>>(h, W, H, pitch, flag);
   return cudaGetLastError();
 }
 

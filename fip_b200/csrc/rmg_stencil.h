@@ -67,6 +67,10 @@ int volume_partials(const StencilState& st);
 cudaError_t launch_volume(const StencilState& st, int parity, double* partials, double* out,
                           cudaStream_t stream);
 
+// Sets *flag (device) to 1 when one of the W x H cells of h (row pitch `pitch` floats) is
+// negative; leaves it as it is otherwise.
+cudaError_t launch_flag_negative(const float* h, int W, int H, int pitch, int* flag, cudaStream_t stream);
+
 // Gathers n sample values (type 0..3 = z, h, qx, qy; z adds terrain) of buffer `parity`.
 cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, const int* xy_type,
                                  float* out, cudaStream_t stream);

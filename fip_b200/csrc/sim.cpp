@@ -785,14 +785,14 @@ int fip_set_field(fip_handle* h, int field, const float* src) {
     ck(cudaMemcpy2DAsync(bufs[p ^ 1], pb, bufs[p], pb, W * 4, H, cudaMemcpyDeviceToDevice, h->stream),
        "fip_set_field");
     if (field == FIP_FIELD_H && !h->h_ctl->hmax_full) {
-      bool negative = false;
-      for (size_t i = 0; i < W * H && !negative; ++i) negative = src[i] < 0.f;
-      if (negative) {
-        h->h_ctl->hmax_full = 1;
-        ck(cudaMemcpyAsync(&h->d_ctl->hmax_full, &h->h_ctl->hmax_full, sizeof(int), cudaMemcpyHostToDevice,
-                           h->stream),
-           "fip_set_field");
-      }
+      // a negative depth anywhere makes the hmax fold cover inactive tiles too; the check runs on
+      // the copy in device memory (a host scan of the caller's buffer costs tens of ms on large
+      // grids) and the flag comes back into the host mirror before this call returns
+      ck(fip::launch_flag_negative(bufs[p], (int)W, (int)H, h->st.pitch, &h->d_ctl->hmax_full, h->stream),
+         "fip_set_field");
+      ck(cudaMemcpyAsync(&h->h_ctl->hmax_full, &h->d_ctl->hmax_full, sizeof(int), cudaMemcpyDeviceToHost,
+                         h->stream),
+         "fip_set_field");
     }
     h->replan = true;
     ck(cudaStreamSynchronize(h->stream), "fip_set_field");
