@@ -104,8 +104,10 @@ int fip_get_field(fip_handle* h, int field, float* host_out);
 /* Replaces one field of the current state (FIP_FIELD_H, _QX or _QY) from a host buffer of W*H
  * floats, in both ping-pong buffers like initDeviceBuffers does for the initial state
  * (src/simdata.cpp:82-88); the active tiles are re-planned before the next step. Pinned host
- * memory makes the copy asynchronous-fast. No counterpart in the reference (which restarts only
- * from files at start-up). */
+ * memory lets the copy run at the host link's speed. A negative depth in an FIP_FIELD_H upload
+ * switches the max-depth fold to the whole grid, as a negative initial depth does at fip_init
+ * (checked on the device copy). Returns once the copy is complete, so the caller may reuse the
+ * buffer. No counterpart in the reference (which restarts only from files at start-up). */
 int fip_set_field(fip_handle* h, int field, const float* host_src);
 
 /* duration (s, FP64), dt of the next step, completed iterations (SimData::duration/dt/iteration). */
