@@ -256,6 +256,15 @@ def surrogate_measure(args):
     return out
 
 
+def workload_config(W, H, world):
+    """The `config` object of both arms' lines: the same workload, whichever arm measures it."""
+    return {"workload": f"scenario1 large grid {W}x{H}, dx 3 m, kSt_var, no_data border, "
+                        "variable dt, q inflow + open bottom; every tile computed",
+            "grid_cells": W * H, "bytes_per_cell": BYTES_PER_CELL,
+            "l2": "working set 1.18 GB per step >> 126 MB L2 (no flush needed)",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -266,7 +275,7 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt / n * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"scenario1 {args.W}x{args.H} (row band, host cores)", "impl": "oracle port"},
+            "config": workload_config(args.W, args.H, world),
             "impl": "reference", "cpu_baseline": res,
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -363,11 +372,7 @@ def run_gpu(args, rank, world, local_rank):
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"scenario1 large grid {W}x{H}, dx 3 m, kSt_var, no_data border, "
-                                       "variable dt, q inflow + open bottom; every tile computed",
-                           "grid_cells": cells, "bytes_per_cell": BYTES_PER_CELL,
-                           "l2": "working set 1.18 GB per step >> 126 MB L2 (no flush needed)",
-                           "parallelism": f"replicas x{world}"},
+                "config": workload_config(W, H, world),
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 3 * cells * 4,
                         "d2h_bytes_per_step": 3 * cells * 4,
                         "note": f"each e2e step = upload h,qx,qy from pinned host + {inner} solver steps + download"},
