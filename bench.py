@@ -65,56 +65,99 @@ def profile_traffic():
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """SM clock, power and throttle reasons sampled during the timed region: NVML read-only
+    queries every 2 ms from a thread (a timed region of a few milliseconds still gets samples),
+    else nvidia-smi every 100 ms."""
+
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
-        self._p = None
+        self.samples = []  # (sm_mhz, sm_max_mhz, power_w, reasons tuple)
+        self._stop = threading.Event()
+        self._t = None
+        self.source = None
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            dev = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(dev, pynvml.NVML_CLOCK_SM)
+
+            def read():
+                sm = pynvml.nvmlDeviceGetClockInfo(dev, pynvml.NVML_CLOCK_SM)
+                pw = pynvml.nvmlDeviceGetPowerUsage(dev) / 1000.0
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(dev)
+                return (float(sm), float(mx), pw, tuple(n for n, b in zip(self.NAMES, bits) if r & b))
+
+            read()
+            self.source = "nvml 2 ms"
+            self._read = read
+            self._t = threading.Thread(target=self._poll_nvml, daemon=True)
+            self._t.start()
+        except Exception:
+            self._start_smi()
+        return self
+
+    def _poll_nvml(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self._read())
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def _start_smi(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
         try:
             self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
                                         "--format=csv,noheader,nounits", "-lms", "100"],
                                        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
-            t0 = time.time()  # keep nvidia-smi's start-up out of the timed region
-            while not self.samples and time.time() - t0 < 10:
-                time.sleep(0.05)
         except Exception:
-            self._p = None
-        self.first = len(self.samples)
-        return self
+            return
+        self.source = "nvidia-smi 100 ms"
 
-    def _read(self):
-        for line in self._p.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 8:
-                self.samples.append(parts)
+        def reader():
+            for line in self._p.stdout:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 7:
+                    try:
+                        self.samples.append((float(p[0]), float(p[1]), float(p[2]),
+                                             tuple(n for n, v in zip(self.NAMES, p[3:7]) if v.lower() == "active")))
+                    except ValueError:
+                        pass
+
+        self._t = threading.Thread(target=reader, daemon=True)
+        self._t.start()
+        t0 = time.time()  # keep nvidia-smi's start-up out of the timed region
+        while not self.samples and time.time() - t0 < 10:
+            time.sleep(0.05)
 
     def __exit__(self, *exc):
-        self.last = len(self.samples)
-        if self._p:
+        self._stop.set()
+        if getattr(self, "_p", None):
             self._p.terminate()
             try:
                 self._p.wait(timeout=5)
             except Exception:
                 self._p.kill()
+        if self._t is not None:
+            self._t.join(timeout=2)
 
     def summary(self):
-        during = self.samples[max(0, self.first - 1):max(self.last, self.first)]
-        if not during:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(s[1]) for s in during if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in during if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in during for i in range(4) if s[4 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(during)}
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples),
+                "power_w_max": max(s[2] for s in self.samples),
+                "reasons": sorted({r for s in self.samples for r in s[3]}),
+                "samples": len(self.samples), "source": self.source}
 
 
 def make_workload(args, rank):
@@ -256,27 +299,43 @@ def surrogate_measure(args):
     return out
 
 
-def workload_config(W, H, world):
+def workload_config(W, H):
     """The `config` object of both arms' lines: the same workload, whichever arm measures it."""
     return {"workload": f"scenario1 large grid {W}x{H}, dx 3 m, kSt_var, no_data border, "
-                        "variable dt, q inflow + open bottom; every tile computed",
-            "grid_cells": W * H, "bytes_per_cell": BYTES_PER_CELL,
-            "l2": "working set 1.18 GB per step >> 126 MB L2 (no flush needed)",
-            "parallelism": f"replicas x{world}"}
+                        "variable dt, q inflow + open bottom; every cell computed",
+            "grid_cells": W * H, "bytes_per_cell": BYTES_PER_CELL}
 
 
 def run_reference(args, rank, world):
+    """The reference's algorithm on the host cores: the whole scenario (every cell, its boundary
+    conditions and variable dt), FP64 restatement of the reference's kernel with all host
+    threads. The reference's own path is CUDA only (no CPU implementation exists)."""
     if rank != 0:
         return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
     sc = make_workload(args, rank)
-    budget = 120.0  # seconds for warmup + steps
-    res, n, dt = cpu_baseline(sc, budget * args.steps / max(args.steps + args.warmup, 1), steps_hint=args.steps)
-    value = res["value"]
+    threads = os.cpu_count() or 1
+    pitch = ((sc.W * 4 + 511) // 512) * 128  # cudaMallocPitch's 512-byte row alignment
+    o = pyoracle.Oracle.from_yaml(sc.yaml_path, pitch, precision=64)
+    o.set_threads(threads)
+    o.simulate(max(args.warmup, 1))
+    t0 = time.perf_counter()
+    o.simulate(args.steps)
+    dt = time.perf_counter() - t0
+    value = sc.W * sc.H * args.steps / dt
+    cpu = {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+           "sample": f"FP64 oracle (restatement of the reference's kernel, boundary conditions and dt control), "
+                     f"whole {sc.W}x{sc.H} grid, {args.steps} steps after {max(args.warmup, 1)} warm-up steps, "
+                     f"{dt:.1f} s, {threads} threads"}
+    cfg = workload_config(sc.W, sc.H)
+    cfg["arm"] = "CPU: FP64 oracle port on the host cores (the reference has no CPU path)"
+    cfg["parallelism"] = f"{threads} host threads"
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dt / n * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(args.W, args.H, world),
-            "impl": "reference", "cpu_baseline": res,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "impl": "reference", "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -323,22 +382,25 @@ def run_gpu(args, rank, world, local_rank):
     value = world * cells * args.steps / (total_ms / 1e3)
 
     # ---- e2e through the C ABI with pinned host buffers ----
+    # every e2e step: the state (h, qx, qy) from pinned host buffers, `inner` solver steps, the
+    # state back into pinned host buffers; the pipelined exchange (fip_stage_state /
+    # fip_step_exchange) overlaps the next upload and the last download with the steps
     inner = args.e2e_inner
-    hbuf = {k: torch.empty((H, W), dtype=torch.float32, pin_memory=True).numpy() for k in ("h", "qx", "qy")}
-    for k in hbuf:
-        sim.field(k, out=hbuf[k])
-    reps = max(1, args.steps // inner)
-    for k in hbuf:  # warm the path once
-        sim.set_field(k, hbuf[k])
-    sim.step(inner)
+    pin = lambda: torch.empty((H, W), dtype=torch.float32, pin_memory=True).numpy()
+    hin = [sim.field(k, out=pin()) for k in ("h", "qx", "qy")]
+    hout = [[pin() for _ in range(3)] for _ in range(2)]
+    reps = max(args.e2e_reps, args.steps // inner)
+    sim.stage_state(*hin)  # warm the path once
+    sim.step_exchange(inner, hout[0])
+    sim.exchange_wait()
     replicas.barrier(dist)
     t0 = time.perf_counter()
-    for _ in range(reps):
-        for k in ("h", "qx", "qy"):
-            sim.set_field(k, hbuf[k])
-        sim.step(inner)
-        for k in ("h", "qx", "qy"):
-            sim.field(k, out=hbuf[k])
+    sim.stage_state(*hin)
+    for i in range(reps):
+        if i + 1 < reps:
+            sim.stage_state(*hin)
+        sim.step_exchange(inner, hout[i % 2])
+    sim.exchange_wait()
     e2e_s = time.perf_counter() - t0
     e2e_s = replicas.max_over_ranks(dist, e2e_s, device="cuda")
     e2e_value = world * cells * inner * reps / e2e_s
@@ -372,10 +434,13 @@ def run_gpu(args, rank, world, local_rank):
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": workload_config(W, H, world),
+                "config": dict(workload_config(W, H), parallelism=f"replicas x{world}",
+                               l2="working set 1.18 GB per step >> 126 MB L2 (no flush needed)"),
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 3 * cells * 4,
                         "d2h_bytes_per_step": 3 * cells * 4,
-                        "note": f"each e2e step = upload h,qx,qy from pinned host + {inner} solver steps + download"},
+                        "note": f"{reps} e2e steps, each = upload of h,qx,qy from pinned host + {inner} solver "
+                                "steps + download into pinned host (fip_stage_state / fip_step_exchange: the "
+                                "copies of one e2e step overlap the solver steps of its neighbours)"},
                 "gpu_launches": 2 * args.steps, "roofline": roof, "clocks": clocks,
                 "cpu_baseline": base, "active_tiles": active, "ensemble": ens, "surrogate": sgm}
         print(json.dumps(line), flush=True)
@@ -393,6 +458,7 @@ def main():
     ap.add_argument("--H", type=int, default=6500)
     ap.add_argument("--spinup", type=float, default=7200.0, help="simulated s before the active-tile measurement")
     ap.add_argument("--e2e-inner", type=int, default=100)
+    ap.add_argument("--e2e-reps", type=int, default=8, help="e2e steps (at least; more when --steps is larger)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ens-members", type=int, default=64, help="batched-ensemble measurement (0: skip)")

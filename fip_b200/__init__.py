@@ -70,6 +70,38 @@ class Simulation:
         assert a.shape == (self.H, self.W)
         _lib.check(_lib.lib().fip_set_field(self._h, FIELDS[name], a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
 
+    # -- pipelined state exchange ----------------------------------------------------------
+    def stage_state(self, h: np.ndarray, qx: np.ndarray, qy: np.ndarray) -> None:
+        """Queues the upload of a whole state (fip_stage_state); the arrays are kept alive until
+        the step_exchange that takes them returns."""
+        arrs = []
+        for a in (h, qx, qy):
+            assert a.dtype == np.float32 and a.shape == (self.H, self.W) and a.flags.c_contiguous
+            arrs.append(a)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _lib.check(_lib.lib().fip_stage_state(self._h, *(a.ctypes.data_as(fp) for a in arrs)))
+        self._staged = getattr(self, "_staged", []) + [arrs]
+
+    def step_exchange(self, n: int, out=None) -> None:
+        """Takes the oldest staged state, runs n steps and queues the download of the state into
+        `out` = (h, qx, qy) arrays (complete after the next call or exchange_wait)."""
+        fp = ctypes.POINTER(ctypes.c_float)
+        if out is None:
+            ptrs = (None, None, None)
+        else:
+            for a in out:
+                assert a.dtype == np.float32 and a.shape == (self.H, self.W) and a.flags.c_contiguous
+            ptrs = tuple(a.ctypes.data_as(fp) for a in out)
+        _lib.check(_lib.lib().fip_step_exchange(self._h, int(n), *ptrs))
+        staged = getattr(self, "_staged", [])
+        if staged:
+            staged.pop(0)
+        self._pending = getattr(self, "_pending", [])[-1:] + ([out] if out is not None else [])
+
+    def exchange_wait(self) -> None:
+        _lib.check(_lib.lib().fip_exchange_wait(self._h))
+        self._pending = []
+
     def volume(self) -> float:
         v = ctypes.c_double()
         _lib.check(_lib.lib().fip_volume(self._h, ctypes.byref(v)))

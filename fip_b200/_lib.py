@@ -34,7 +34,8 @@ EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_ru
            "fip_ensemble_destroy", "fip_checkpoint", "fip_restore", "fip_render", "fip_ensemble_render",
            "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad", "fip_ensemble_gather", "fip_sg_pack_input", "fip_sg_target",
            "fip_sg_loss", "fip_sg_bias_grad", "fip_sg_adamw", "fip_sg_cast_weights", "fip_sg_apply",
-           "fip_sg_edge_flux", "fip_sg_pin", "fip_sg_edges", "fip_inject_wait_timeout")
+           "fip_sg_edge_flux", "fip_sg_pin", "fip_sg_edges", "fip_inject_wait_timeout", "fip_stage_state",
+           "fip_step_exchange", "fip_exchange_wait")
 
 
 class FipOptions(ctypes.Structure):
@@ -91,6 +92,9 @@ def lib():
         L.fip_volume.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.fip_get_field.argtypes = [vp, ip, fp]
         L.fip_set_field.argtypes = [vp, ip, fp]
+        L.fip_stage_state.argtypes = [vp, fp, fp, fp]
+        L.fip_step_exchange.argtypes = [vp, ip, fp, fp, fp]
+        L.fip_exchange_wait.argtypes = [vp]
         L.fip_time.argtypes = [vp, ctypes.POINTER(ctypes.c_double), fp, ctypes.POINTER(ctypes.c_int)]
         L.fip_info.argtypes = [vp, ctypes.POINTER(FipInfo)]
         L.fip_profile_steps.argtypes = [vp, ip, fp, fp]

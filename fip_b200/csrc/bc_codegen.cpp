@@ -3,6 +3,7 @@
 #include <nvrtc.h>
 
 #include "drv.h"
+#include "rmg_stencil.h"
 
 #include <cstdio>
 #include <cstring>
@@ -484,6 +485,30 @@ void emit_cells(std::ostream& o, const BoundaryCondition& bc, bool staggered, lo
 }
 
 }  // namespace
+
+void bc_tile_force(const Config& cfg, TileForce* out) {
+  // A condition writes, at every position from..to along its side, the side's cell, the inner
+  // neighbour and the staggered face: cells within 1 of the edge. The step reads 2 cells around
+  // every cell it updates, so the tiles within 3 cells of those are kept active; the margin used
+  // is 4 along the side and 6 cells deep.
+  constexpr int kAlong = 4, kDeep = 6;
+  *out = TileForce{};
+  if (cfg.bcs.size() > (size_t)kMaxForceRects) {
+    out->all_band = 1;
+    return;
+  }
+  const int W = (int)cfg.W, H = (int)cfg.H;
+  for (const BoundaryCondition& bc : cfg.bcs) {
+    int* r = out->rect[out->n++];
+    const int a0 = bc.from - kAlong, a1 = bc.to + kAlong;
+    switch (bc.side) {
+      case BcSide::left: r[0] = 0; r[1] = kDeep - 1; r[2] = a0; r[3] = a1; break;
+      case BcSide::right: r[0] = W - kDeep; r[1] = W - 1; r[2] = a0; r[3] = a1; break;
+      case BcSide::bottom: r[0] = a0; r[1] = a1; r[2] = 0; r[3] = kDeep - 1; break;
+      default: r[0] = a0; r[1] = a1; r[2] = H - kDeep; r[3] = H - 1; break;  // top
+    }
+  }
+}
 
 SeriesLayout layout_series(const Config& cfg) {
   SeriesLayout s;

@@ -15,6 +15,8 @@
 
 namespace fip {
 
+struct TileForce;  // rmg_stencil.h
+
 struct SeriesLayout {
   std::vector<float> data;      // concatenated tables, uploaded to the device
   std::vector<long> z_off, q_off;  // per condition: offset of its z / q table (-1: none)
@@ -22,6 +24,12 @@ struct SeriesLayout {
 };
 
 SeriesLayout layout_series(const Config& cfg);
+
+// The cells each boundary condition of `cfg` writes (the side's cell, its inner neighbour and the
+// staggered face of every position from..to, src/bc_kernel_gen.cpp:10-136), widened by the
+// stencil's reach: their tiles are always computed. Tiles elsewhere on the edge are computed
+// only while they or their neighbours hold water.
+void bc_tile_force(const Config& cfg, TileForce* out);
 
 // CUDA source of the post kernel for `cfg` (pitch in elements: the top/bottom open boundary
 // scales its outflow by idx - idx_neighbor = +-pitch, src/bc_kernel_gen.cpp:122, :132).

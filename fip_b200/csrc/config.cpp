@@ -134,8 +134,9 @@ BcSide bc_side(const std::string& s) { return enum_of<BcSide>(s, {"left", "right
 SampleType sample_type(const std::string& s) { return enum_of<SampleType>(s, {"z", "h", "qx", "qy"}); }
 Solver solver_of(const std::string& s) { return enum_of<Solver>(s, {"rmg", "cn"}); }
 
-// validateSimDataConfig (src/simdata.cpp:152-236), same messages
-bool validate(const YNode& config) {
+// validateSimDataConfig (src/simdata.cpp:152-236), same messages; `quiet` drops the warnings
+// (never the errors)
+bool validate(const YNode& config, bool quiet) {
   bool ok = true;
   auto error = [&ok](const YNode& node, const std::string& msg) {
     ok = false;
@@ -158,7 +159,7 @@ bool validate(const YNode& config) {
   for (const char* k : {"name", "terrain", "W", "H", "dt", "dx", "duration"}) in_config(config, k);
   xor_in_config(config, "kSt_var", "kSt");
   for (const char* k : {"terrain", "z", "qx", "qy", "kSt_var"}) good_path(config, k);
-  if (!config["kSt_var"].defined() && !config["kSt"].defined())
+  if (!quiet && !config["kSt_var"].defined() && !config["kSt"].defined())
     std::cerr << "Warning: both \"kSt_var\" and \"kSt\" missing, using default kSt " << 30.f << std::endl;
   for (const YNode& bc : config["boundary_conditions"].seq()) {
     in_config(bc, "side");
@@ -181,7 +182,7 @@ bool validate(const YNode& config) {
     for (const YNode& sp : config["sampling"].seq())
       for (const char* k : {"x", "y", "label", "type"}) in_config(sp, k);
   }
-  if (!config["save_state"].defined()) std::cerr << "Warning: no save_state times given" << std::endl;
+  if (!quiet && !config["save_state"].defined()) std::cerr << "Warning: no save_state times given" << std::endl;
   return ok;
 }
 
@@ -206,12 +207,12 @@ std::vector<float> load_grid(const YNode& node, size_t W, size_t H) {
 
 }  // namespace
 
-int load_config(const std::string& path, Config* out, std::string* err) {
+int load_config(const std::string& path, Config* out, std::string* err, bool quiet) {
   Config c;
   c.yaml_path = path;
   try {
     YNode config = YNode::load_file(path);
-    if (!validate(config)) throw std::invalid_argument("one or more configuration errors found");
+    if (!validate(config, quiet)) throw std::invalid_argument("one or more configuration errors found");
     c.name = config["name"].as_string();
     c.target_duration = solve_simple_math(config["duration"].as_string());
     long long W = config["W"].as_int64(), H = config["H"].as_int64();

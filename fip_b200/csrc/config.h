@@ -73,7 +73,8 @@ double solve_simple_math(const std::string& expr);
 // Loads and validates a parameter file (SimData::loadSimData, src/simdata.cpp:238-310).
 // Validation messages and warnings go to stderr with the reference's wording; on failure the
 // return value is nonzero and *err holds the message the reference's main() prints after
-// "Config error: ". Returns 2 for I/O errors on the input files.
-int load_config(const std::string& path, Config* out, std::string* err);
+// "Config error: ". Returns 2 for I/O errors on the input files. With `quiet` the warnings (no
+// save_state times, default kSt) are not printed; errors always are.
+int load_config(const std::string& path, Config* out, std::string* err, bool quiet = false);
 
 }  // namespace fip

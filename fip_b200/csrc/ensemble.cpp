@@ -213,6 +213,7 @@ void fip_ensemble::init(const std::vector<std::string>& paths, const fip_options
       // arithmetic in both forms of the kernel
       if (c.has_kst_var) up(st.kst, c.kst);
       else up(st.kst, std::vector<float>(W * H, c.kst_fixed));
+      eck(fip::prepare_kst_field(st.kst + off, (int)W, (int)H, pitch, stream), "kst");
     }
   }
   st.W = packed_W;
@@ -335,11 +336,13 @@ void fip_ensemble::set_shape(Shape s, bool replan) {
     const FipEnsMember& M = mem[m];
     const size_t off = (size_t)M.row_off * pitch;
     const bool other = replan;  // after steps the partner buffer may still hold water elsewhere
+    fip::TileForce force;
+    fip::bc_tile_force(*cfgs[m], &force);
     eck(fip::launch_init_tiles_region(st.h[par] + off, st.qx[par] + off, st.qy[par] + off,
                                       other ? st.h[par ^ 1] + off : nullptr, other ? st.qx[par ^ 1] + off : nullptr,
                                       other ? st.qy[par ^ 1] + off : nullptr, st.sohle + off, M.W, M.H, pitch,
-                                      M.no_value, tc, s.tile_rows, st.sticky + M.tile_base, nz_cur + M.tile_base,
-                                      nz_prev + M.tile_base, stream),
+                                      M.no_value, tc, s.tile_rows, force, st.sticky + M.tile_base,
+                                      nz_cur + M.tile_base, nz_prev + M.tile_base, stream),
         "init_tiles");
   }
   if (replan) launch_post(FIP_POST_MODE_PLAN);
@@ -495,7 +498,7 @@ int fip_ensemble_init(const char* const* yaml_paths, int n_members, const fip_op
     paths.emplace_back(yaml_paths[m]);
     std::unique_ptr<fip::Config> c(new fip::Config());
     std::string err;
-    const int rc = fip::load_config(paths.back(), c.get(), &err);
+    const int rc = fip::load_config(paths.back(), c.get(), &err, o.quiet != 0);
     if (rc == 2) return efail(FIP_ERR_IO, paths.back() + ": " + err);
     if (rc) return efail(FIP_ERR_CONFIG, paths.back() + ": " + err);
     if (c->W < 4 || c->H < 4) return efail(FIP_ERR_CONFIG, paths.back() + ": grids must be at least 4 x 4 cells");

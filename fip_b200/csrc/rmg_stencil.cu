@@ -197,6 +197,39 @@ __device__ __forceinline__ void vfma(float (&d)[4], float2 a, const float (&b)[4
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
 
+#ifndef FIP_VAR_MAX3
+#define FIP_VAR_MAX3 0
+#endif
+#ifndef FIP_VAR_IK2
+#define FIP_VAR_IK2 0
+#endif
+#ifndef FIP_VAR_POW
+#define FIP_VAR_POW 0
+#endif
+// max(a, b, c) in one instruction (sm_100 three-input max), flush-to-zero like fmaxf under
+// -use_fast_math
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+#if FIP_VAR_MAX3
+  float r;
+  asm("max.ftz.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+#else
+  return fmaxf(fmaxf(a, b), c);
+#endif
+}
+// (1 / a)^2.33 of the friction factor
+__device__ __forceinline__ float pow_inv(float a) {
+#if FIP_VAR_POW
+  float l, r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(a));
+  l *= -2.33f;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l));
+  return r;
+#else
+  return powf(1.f / a, 2.33f);
+#endif
+}
+
 template <int FB = kFieldBytes>
 __device__ __forceinline__ float4 lds4(const unsigned char* slot, int field, int col) {
   return *reinterpret_cast<const float4*>(slot + field * FB + col * 4);
@@ -556,9 +589,9 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       const float hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        uyS[k] = qyS[k] / fmaxf(fmaxf(kDH, hs[k]), h0[k]);
-        ux0[k] = qx0[k] / fmaxf(fmaxf(kDH, h0[k]), k < 3 ? h0[k + 1] : hE0);
-        uy0[k] = qy0[k] / fmaxf(fmaxf(kDH, h0[k]), h1[k]);
+        uyS[k] = qyS[k] / fmax3(kDH, hs[k], h0[k]);
+        ux0[k] = qx0[k] / fmax3(kDH, h0[k], k < 3 ? h0[k + 1] : hE0);
+        uy0[k] = qy0[k] / fmax3(kDH, h0[k], h1[k]);
       }
       vmul(lim0, h0, c_dti);
       vmul(lim0, lim0, c_dx);
@@ -615,9 +648,14 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
         if (KVAR) {
           const float4 vk = lds4<kFB>(sl0, F_K, scol);
           float kk[4] = {vk.x, vk.y, vk.z, vk.w};
+#if FIP_VAR_IK2
+          const float g = ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg;  // the field holds 1 / kSt^2
+          vmul(fric, kk, make_float2(g, g));
+#else
           vmul(kk, kk, kk);
 #pragma unroll
           for (int k = 0; k < 4; ++k) fric[k] = (ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg) / kk[k];
+#endif
         } else {
           fric[0] = fric[1] = fric[2] = fric[3] = ENS ? ldsf_at_use(&s_mcf[warp][10]) : fric_u;
         }
@@ -635,8 +673,8 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       float ux1[4], uy1[4], lim1[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        ux1[k] = qx1[k] / fmaxf(fmaxf(kDH, h1[k]), k < 3 ? h1[k + 1] : hE1);
-        uy1[k] = qy1[k] / fmaxf(fmaxf(kDH, h1[k]), h2r[k]);
+        ux1[k] = qx1[k] / fmax3(kDH, h1[k], k < 3 ? h1[k + 1] : hE1);
+        uy1[k] = qy1[k] / fmax3(kDH, h1[k], h2r[k]);
       }
       vmul(lim1, h1, ENS ? lds2_at_use(&s_mcf[warp][0]) : c_dti);
       vmul(lim1, lim1, ENS ? lds2_at_use(&s_mcf[warp][2]) : c_dx);
@@ -713,14 +751,14 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           t[k] = sqrtf(mx[k]);
-          u[k] = powf(1.f / ax1[k], 2.33f);
+          u[k] = pow_inv(ax1[k]);
         }
         vmul(rx, fric, t);
         vmul(rx, rx, u);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           t[k] = sqrtf(my[k]);
-          u[k] = powf(1.f / ay1[k], 2.33f);
+          u[k] = pow_inv(ay1[k]);
         }
         vmul(ry, fric, t);
         vmul(ry, ry, u);
@@ -953,34 +991,59 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
 // Per tile of a tile_cols x tile_rows grid: sticky flag and whether buffer (h, qx, qy) has a
 // nonzero cell (into nz0 and nz1). With or_into set, the nonzero flag is OR-ed into or_into[t]
 // instead and nothing else is written.
+// A tile is sticky (computed every step) when
+//  * a cell the step never writes holds water within 2 cells of it (the step reads 2 cells
+//    around each cell it updates): no_data cells, and the cells within 1 of the edge that the
+//    reference's write sets leave out (src/kernels.cu:383-406) -- only boundary conditions change
+//    those, and the conditions' own cells are covered next;
+//  * it meets a rectangle of `force`: the cells a boundary condition writes, widened by the
+//    stencil's reach (or, with force.all_band, any tile within 4 cells of the edge).
+// Elsewhere a tile whose 3 x 3 neighbourhood is all zero computes zeros, which the plan exploits.
 __global__ void init_tiles_kernel(const float* h, const float* qx, const float* qy, const float* sohle, int W, int H,
                                   int pitch, float no_value, int n_ty, int n_tiles, int tile_cols, int tile_rows,
-                                  unsigned char* or_into, unsigned char* sticky, unsigned char* nz0,
-                                  unsigned char* nz1) {
+                                  const TileForce force, unsigned char* or_into, unsigned char* sticky,
+                                  unsigned char* nz0, unsigned char* nz1) {
   const int t = blockIdx.x;
   if (t >= n_tiles) return;
   const int s = t / n_ty, ty = t - s * n_ty;
   const int c0 = s * tile_cols, r0 = ty * tile_rows;
   const int c1 = min(c0 + tile_cols, W), r1 = min(r0 + tile_rows, H);
   int nz = 0, st = 0;
-  for (int e = threadIdx.x; e < tile_cols * tile_rows; e += blockDim.x) {
-    const int r = r0 + e / tile_cols, c = c0 + e % tile_cols;
-    if (r < r1 && c < c1) {
-      const size_t o = (size_t)r * pitch + c;
-      const bool nzc = (h[o] != 0.f) || (qx[o] != 0.f) || (qy[o] != 0.f);
-      nz |= nzc;
-      if (sohle[o] == no_value && nzc) st = 1;  // never written by the step: static water
-    }
-  }
-  // border band: boundary conditions write within 2 cells of the edge and the stencil reads
-  // 2 cells further, so tiles reaching within 4 cells of an edge are always computed
-  if (r0 < 4 || r1 > H - 4 || c0 < 4 || c1 > W - 4) st = 1;
-  nz = __syncthreads_or(nz);
-  st = __syncthreads_or(st);
   if (or_into) {
+    for (int e = threadIdx.x; e < tile_cols * tile_rows; e += blockDim.x) {
+      const int r = r0 + e / tile_cols, c = c0 + e % tile_cols;
+      if (r < r1 && c < c1) {
+        const size_t o = (size_t)r * pitch + c;
+        nz |= (h[o] != 0.f) || (qx[o] != 0.f) || (qy[o] != 0.f);
+      }
+    }
+    nz = __syncthreads_or(nz);
     if (threadIdx.x == 0 && nz) or_into[t] = 1;
     return;
   }
+  // the tile widened by the stencil's reach of 2 cells, clipped to the grid
+  const int x0 = max(c0 - 2, 0), x1 = min(c1 + 2, W), y0 = max(r0 - 2, 0), y1 = min(r1 + 2, H);
+  const int ww = x1 - x0;
+  for (int e = threadIdx.x; e < ww * (y1 - y0); e += blockDim.x) {
+    const int r = y0 + e / ww, c = x0 + e % ww;
+    const size_t o = (size_t)r * pitch + c;
+    const bool nzc = (h[o] != 0.f) || (qx[o] != 0.f) || (qy[o] != 0.f);
+    if (r >= r0 && r < r1 && c >= c0 && c < c1) nz |= nzc;
+    const bool unwritten = r <= 1 || r >= H - 2 || c <= 1 || c >= W - 2 || sohle[o] == no_value;
+    if (nzc && unwritten) st = 1;
+  }
+  if (threadIdx.x == 0) {
+    if (force.all_band) {
+      if (r0 < 4 || r1 > H - 4 || c0 < 4 || c1 > W - 4) st = 1;
+    } else {
+      for (int i = 0; i < force.n; ++i) {
+        const int* q = force.rect[i];
+        if (q[0] < c1 && q[1] >= c0 && q[2] < r1 && q[3] >= r0) st = 1;
+      }
+    }
+  }
+  nz = __syncthreads_or(nz);
+  st = __syncthreads_or(st);
   if (threadIdx.x == 0) {
     sticky[t] = (unsigned char)st;
     nz0[t] = (unsigned char)nz;
@@ -1084,6 +1147,26 @@ int make_tensor_maps(StencilState* st) {
   return 0;
 }
 
+#if FIP_VAR_IK2
+__global__ void kst_inverse_kernel(float* k, int W, int H, int pitch) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  if (c < W && r < H) {
+    const size_t o = (size_t)r * pitch + c;
+    k[o] = 1.f / (k[o] * k[o]);
+  }
+}
+#endif
+
+cudaError_t prepare_kst_field(float* kst, int W, int H, int pitch, cudaStream_t stream) {
+#if FIP_VAR_IK2
+  if (!kst) return cudaSuccess;
+  kst_inverse_kernel<<<dim3((W + 255) / 256, H), 256, 0, stream>>>(kst, W, H, pitch);
+  return cudaGetLastError();
+#else
+  return cudaSuccess;
+#endif
+}
+
 int rmg_step_grid(int device) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1157,23 +1240,24 @@ int rmg_step_grid_kw(int device, int kw) {
 cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t stream) {
   init_tiles_kernel<<<st.n_tiles, 256, 0, stream>>>(st.h[parity], st.qx[parity], st.qy[parity], st.sohle, st.W, st.H,
                                                     st.pitch, st.no_value, st.n_ty, st.n_tiles, FIP_TILE_COLS,
-                                                    FIP_TILE_ROWS, nullptr, st.sticky, st.nz[0], st.nz[1]);
+                                                    FIP_TILE_ROWS, st.force, nullptr, st.sticky, st.nz[0], st.nz[1]);
   return cudaGetLastError();
 }
 
 cudaError_t launch_init_tiles_region(const float* h, const float* qx, const float* qy, const float* h_other,
                                      const float* qx_other, const float* qy_other, const float* sohle, int W, int H,
-                                     int pitch, float no_value, int tile_cols, int tile_rows, unsigned char* sticky,
-                                     unsigned char* nz_cur, unsigned char* nz_prev, cudaStream_t stream) {
+                                     int pitch, float no_value, int tile_cols, int tile_rows, const TileForce& force,
+                                     unsigned char* sticky, unsigned char* nz_cur, unsigned char* nz_prev,
+                                     cudaStream_t stream) {
   const int n_sx = (W + tile_cols - 1) / tile_cols, n_ty = (H + tile_rows - 1) / tile_rows;
   init_tiles_kernel<<<n_sx * n_ty, 256, 0, stream>>>(h, qx, qy, sohle, W, H, pitch, no_value, n_ty, n_sx * n_ty,
-                                                     tile_cols, tile_rows, nullptr, sticky, nz_cur, nz_prev);
+                                                     tile_cols, tile_rows, force, nullptr, sticky, nz_cur, nz_prev);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !h_other) return e;
   // the other buffer becomes the next step's output: a tile must be computed while it is nonzero
   init_tiles_kernel<<<n_sx * n_ty, 256, 0, stream>>>(h_other, qx_other, qy_other, sohle, W, H, pitch, no_value, n_ty,
-                                                     n_sx * n_ty, tile_cols, tile_rows, nz_prev, nullptr, nullptr,
-                                                     nullptr);
+                                                     n_sx * n_ty, tile_cols, tile_rows, force, nz_prev, nullptr,
+                                                     nullptr, nullptr);
   return cudaGetLastError();
 }
 
@@ -1209,9 +1293,9 @@ cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, cons
 // One rmg step without any device allocation (fip_rmg_step_noalloc in include/fip.h).
 //
 // Some callers cannot allocate device memory: a host that drives this step from its own time
-// loop while other streams keep the GPU busy (cudaFree synchronises the whole device), a host
-// that owns all device memory through its own pool and forbids allocations once it runs, or
-// code that records the step into a CUDA graph. For them the step's scratch (control block,
+// loop while other streams keep the GPU busy (cudaFree synchronises the whole device), or a host
+// that owns all device memory through its own pool and forbids allocations once it runs. For
+// them the step's scratch (control block,
 // tile list, per-tile wet flags) lives in the file-scope array below, which every GPU that loads
 // the library holds until the process exits. It holds the plan of at most kNoAllocMaxTiles tiles
 // of 480 x 32 cells (about 503 million cells); larger grids are rejected. All calls share it and
@@ -1254,6 +1338,7 @@ __global__ void noalloc_setup_kernel(unsigned char* scratch, float dt, int n_til
     ctl->hmax_every = 0;
     ctl->hmax_full = 0;
     ctl->force_all = 1;
+    ctl->inject = 0;
     ctl->cfl_bits[0] = ctl->cfl_bits[1] = __float_as_uint(1.0f);
     ctl->post_done = 0u;
   }

@@ -8,6 +8,17 @@
 
 namespace fip {
 
+// Tiles that are always computed because boundary conditions write near them: inclusive cell
+// rectangles (columns c0..c1, rows r0..r1) covering every cell a configured condition writes,
+// widened by the stencil's reach. all_band forces every tile within 4 cells of the edge instead
+// (more conditions than the list holds).
+constexpr int kMaxForceRects = 32;
+struct TileForce {
+  int n = 0;
+  int all_band = 0;
+  int rect[kMaxForceRects][4] = {};  // c0, c1, r0, r1
+};
+
 // Device buffers and planning scratch of one scenario. Fields are cudaMallocPitch'ed like the
 // reference (src/simdata.cpp:63-73): W floats per row, H+3 rows, `pitch` elements per row.
 struct StencilState {
@@ -18,7 +29,7 @@ struct StencilState {
   float* kst;   // nullptr: uniform kst_fixed
   float* hmax;
   FipCtl* ctl;  // device control block
-  unsigned char* sticky;  // per tile: always active (domain border band, static no_data water)
+  unsigned char* sticky;  // per tile: always active (boundary-condition cells, static water on cells the step never writes)
   unsigned char* nz[2];   // per tile: some cell of the new state is nonzero, by iteration parity
   int* list[2];           // active tiles by chunk (front) / inactive tiles (back), by parity
   int* chunk_cnt[2];      // active tiles per chunk, by parity
@@ -32,6 +43,7 @@ struct StencilState {
   int n_members = 0;
   int tile_rows = FIP_TILE_ROWS;
   int kw = 4;  // consumer warps per CTA: tiles of 120 * kw columns
+  TileForce force;  // single grids: tiles the boundary conditions keep active
 };
 
 // Geometry of the tile grid for a W x H domain.
@@ -52,8 +64,9 @@ cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t s
 // output buffer still holds water is computed.
 cudaError_t launch_init_tiles_region(const float* h, const float* qx, const float* qy, const float* h_other,
                                      const float* qx_other, const float* qy_other, const float* sohle, int W, int H,
-                                     int pitch, float no_value, int tile_cols, int tile_rows, unsigned char* sticky,
-                                     unsigned char* nz_cur, unsigned char* nz_prev, cudaStream_t stream);
+                                     int pitch, float no_value, int tile_cols, int tile_rows, const TileForce& force,
+                                     unsigned char* sticky, unsigned char* nz_cur, unsigned char* nz_prev,
+                                     cudaStream_t stream);
 
 // CTAs the step kernel runs with for tiles of kw consumer warps (3 per SM for 4 warps, 5 for 2).
 int rmg_step_grid_kw(int device, int kw);
@@ -74,6 +87,9 @@ cudaError_t launch_flag_negative(const float* h, int W, int H, int pitch, int* f
 // Gathers n sample values (type 0..3 = z, h, qx, qy; z adds terrain) of buffer `parity`.
 cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, const int* xy_type,
                                  float* out, cudaStream_t stream);
+
+// Converts an uploaded kSt grid into the form the step kernel reads.
+cudaError_t prepare_kst_field(float* kst, int W, int H, int pitch, cudaStream_t stream);
 
 // Number of CTAs the step kernel runs with (3 per SM).
 int rmg_step_grid(int device);

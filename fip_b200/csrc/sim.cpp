@@ -86,8 +86,20 @@ struct fip_handle {
   std::map<int, cudaGraphExec_t> graphs;
   std::ostream* out = &std::cout;
   std::unique_ptr<std::ofstream> out_file;
+  // pipelined state exchange (fip_stage_state / fip_step_exchange): two pitched input and two
+  // output slots of (h, qx, qy), a copy-in and a copy-out stream, events between the streams
+  struct Exchange {
+    bool ready = false;
+    cudaStream_t in = nullptr, out = nullptr;
+    float* slot_in[2][3] = {};
+    float* slot_out[2][3] = {};
+    cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_done[2] = {};
+    bool out_pending[2] = {};
+    int head = 0, count = 0, out_next = 0;
+  } x;
 
   ~fip_handle();
+  void exchange_setup();
   void init(const std::string& yaml, const fip_options& o);
   void write_ctl_fields();
   void read_ctl();
@@ -103,6 +115,22 @@ struct fip_handle {
 
 fip_handle::~fip_handle() {
   if (device >= 0) cudaSetDevice(device);
+  if (x.ready) {
+    cudaStreamSynchronize(x.in);
+    cudaStreamSynchronize(x.out);
+    for (int s = 0; s < 2; ++s) {
+      for (int f = 0; f < 3; ++f) {
+        cudaFree(x.slot_in[s][f]);
+        cudaFree(x.slot_out[s][f]);
+      }
+      cudaEventDestroy(x.in_ready[s]);
+      cudaEventDestroy(x.in_free[s]);
+      cudaEventDestroy(x.out_ready[s]);
+      cudaEventDestroy(x.out_done[s]);
+    }
+    cudaStreamDestroy(x.in);
+    cudaStreamDestroy(x.out);
+  }
   for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
   fip::destroy_post_kernel(&post);
   for (int b = 0; b < 2; ++b) {
@@ -168,6 +196,7 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
   up(st.hmax, cfg.h0);
   up(st.sohle, cfg.terrain);
   if (cfg.has_kst_var) up(st.kst, cfg.kst);
+  if (st.kst) ck(fip::prepare_kst_field(st.kst, (int)W, (int)H, pitch, stream), "kst");
 
   st.W = (int)W;
   st.H = (int)H;
@@ -177,6 +206,7 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
   st.no_value = cfg.no_data;
   fip::tile_geometry(st.W, st.H, &st.n_sx, &st.n_ty, &st.n_tiles, &st.n_chunks);
   if (st.n_chunks > 256) throw CudaError("grid too large: more than 131072 tiles");
+  fip::bc_tile_force(cfg, &st.force);
   ck(cudaMalloc((void**)&st.sticky, st.n_tiles), "cudaMalloc");
   for (int b = 0; b < 2; ++b) {
     ck(cudaMalloc((void**)&st.nz[b], st.n_tiles), "cudaMalloc");
@@ -260,6 +290,27 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
     for (const auto& p : cfg.points) *out << p.label << ";";
     *out << std::endl;
   }
+}
+
+// Slots, streams and events of the pipelined exchange, made at its first use.
+void fip_handle::exchange_setup() {
+  if (x.ready) return;
+  const size_t bytes = (size_t)st.pitch * sizeof(float) * (cfg.H + 3);
+  ck(cudaStreamCreateWithFlags(&x.in, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaStreamCreateWithFlags(&x.out, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int s = 0; s < 2; ++s) {
+    for (int f = 0; f < 3; ++f) {
+      ck(cudaMalloc((void**)&x.slot_in[s][f], bytes), "cudaMalloc");
+      ck(cudaMalloc((void**)&x.slot_out[s][f], bytes), "cudaMalloc");
+    }
+    ck(cudaEventCreateWithFlags(&x.in_ready[s], cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&x.in_free[s], cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&x.out_ready[s], cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&x.out_done[s], cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventRecord(x.in_free[s], stream), "cudaEventRecord");
+    ck(cudaEventRecord(x.out_done[s], x.out), "cudaEventRecord");
+  }
+  x.ready = true;
 }
 
 // host-owned control fields: event times, step budget, stop flag
@@ -540,7 +591,7 @@ int fip_init_ex(const char* yaml_path, const fip_options* opt, fip_handle** out)
   if (opt) o = *opt;
   std::unique_ptr<fip_handle> h(new fip_handle());
   std::string err;
-  int rc = fip::load_config(yaml_path, &h->cfg, &err);
+  int rc = fip::load_config(yaml_path, &h->cfg, &err, o.quiet != 0);
   if (rc == 2) return fail(FIP_ERR_IO, err);
   if (rc) return fail(FIP_ERR_CONFIG, err);
   rc = guard([&] {
@@ -700,7 +751,8 @@ int fip_restore(fip_handle* h, const char* path) {
     const int k = hd.iteration - 1;
     ck(fip::launch_init_tiles_region(h->st.h[p], h->st.qx[p], h->st.qy[p], h->st.h[p ^ 1], h->st.qx[p ^ 1],
                                      h->st.qy[p ^ 1], h->st.sohle, h->st.W, h->st.H, h->st.pitch, h->st.no_value,
-                                     FIP_TILE_COLS, FIP_TILE_ROWS, h->st.sticky, h->st.nz[k & 1], h->st.nz[(k + 1) & 1],
+                                     FIP_TILE_COLS, FIP_TILE_ROWS, h->st.force, h->st.sticky, h->st.nz[k & 1],
+                                     h->st.nz[(k + 1) & 1],
                                      h->stream),
        "init_tiles");
     if (h->started) h->launch_post(FIP_POST_MODE_PLAN);
@@ -796,6 +848,98 @@ int fip_set_field(fip_handle* h, int field, const float* src) {
     }
     h->replan = true;
     ck(cudaStreamSynchronize(h->stream), "fip_set_field");
+    return FIP_OK;
+  });
+}
+
+int fip_stage_state(fip_handle* h, const float* h_src, const float* qx_src, const float* qy_src) {
+  if (!h || !h_src || !qx_src || !qy_src) return fail(FIP_ERR_ARG, "null argument");
+  if (h->x.ready && h->x.count == 2) return fail(FIP_ERR_ARG, "fip_stage_state: two states are already staged");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    h->exchange_setup();
+    auto& x = h->x;
+    const int s = (x.head + x.count) & 1;
+    const size_t W = h->cfg.W, H = h->cfg.H, pb = (size_t)h->st.pitch * 4;
+    // the slot's previous contents must have been copied into the state first
+    ck(cudaStreamWaitEvent(x.in, x.in_free[s], 0), "fip_stage_state");
+    const float* src[3] = {h_src, qx_src, qy_src};
+    for (int f = 0; f < 3; ++f)
+      ck(cudaMemcpy2DAsync(x.slot_in[s][f], pb, src[f], W * 4, W * 4, H, cudaMemcpyHostToDevice, x.in),
+         "fip_stage_state");
+    ck(cudaEventRecord(x.in_ready[s], x.in), "fip_stage_state");
+    ++x.count;
+    return FIP_OK;
+  });
+}
+
+int fip_step_exchange(fip_handle* h, int n_steps, float* h_dst, float* qx_dst, float* qy_dst) {
+  if (!h || n_steps < 0) return fail(FIP_ERR_ARG, "bad argument");
+  if ((h_dst || qx_dst || qy_dst) && !(h_dst && qx_dst && qy_dst))
+    return fail(FIP_ERR_ARG, "fip_step_exchange: give all three outputs or none");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    h->exchange_setup();
+    auto& x = h->x;
+    const size_t bytes = (size_t)h->st.pitch * 4 * h->cfg.H;
+    if (x.count > 0) {  // the oldest staged state becomes the current state, in both buffers
+      const int s = x.head;
+      const int p = h->h_ctl->parity;
+      ck(cudaStreamWaitEvent(h->stream, x.in_ready[s], 0), "fip_step_exchange");
+      float* const* bufs[3] = {h->st.h, h->st.qx, h->st.qy};
+      for (int f = 0; f < 3; ++f) {
+        ck(cudaMemcpyAsync(bufs[f][p], x.slot_in[s][f], bytes, cudaMemcpyDeviceToDevice, h->stream), "exchange");
+        ck(cudaMemcpyAsync(bufs[f][p ^ 1], x.slot_in[s][f], bytes, cudaMemcpyDeviceToDevice, h->stream), "exchange");
+      }
+      ck(cudaEventRecord(x.in_free[s], h->stream), "exchange");
+      // a negative depth makes the hmax fold cover inactive tiles (as fip_set_field); the flag
+      // stays on the device, where the stencil reads it
+      ck(fip::launch_flag_negative(h->st.h[p], (int)h->cfg.W, (int)h->cfg.H, h->st.pitch, &h->d_ctl->hmax_full,
+                                   h->stream),
+         "exchange");
+      h->replan = true;
+      x.head ^= 1;
+      --x.count;
+    }
+    int rc = n_steps > 0 ? h->run_steps(n_steps, false) : FIP_OK;
+    if (rc) return rc;
+    // the previous call's downloads end before this call returns
+    const int prev = x.out_next ^ 1;
+    if (h_dst) {
+      const int o = x.out_next;
+      const int p = h->h_ctl->parity;
+      const size_t W = h->cfg.W, H = h->cfg.H, pb = (size_t)h->st.pitch * 4;
+      ck(cudaStreamWaitEvent(h->stream, x.out_done[o], 0), "exchange");
+      const float* cur[3] = {h->st.h[p], h->st.qx[p], h->st.qy[p]};
+      float* dst[3] = {h_dst, qx_dst, qy_dst};
+      for (int f = 0; f < 3; ++f)
+        ck(cudaMemcpyAsync(x.slot_out[o][f], cur[f], bytes, cudaMemcpyDeviceToDevice, h->stream), "exchange");
+      ck(cudaEventRecord(x.out_ready[o], h->stream), "exchange");
+      ck(cudaStreamWaitEvent(x.out, x.out_ready[o], 0), "exchange");
+      for (int f = 0; f < 3; ++f)
+        ck(cudaMemcpy2DAsync(dst[f], W * 4, x.slot_out[o][f], pb, W * 4, H, cudaMemcpyDeviceToHost, x.out),
+           "exchange");
+      ck(cudaEventRecord(x.out_done[o], x.out), "exchange");
+      x.out_pending[o] = true;
+      x.out_next ^= 1;
+    }
+    if (x.out_pending[prev]) {
+      ck(cudaEventSynchronize(x.out_done[prev]), "exchange");
+      x.out_pending[prev] = false;
+    }
+    return FIP_OK;
+  });
+}
+
+int fip_exchange_wait(fip_handle* h) {
+  if (!h) return fail(FIP_ERR_ARG, "null handle");
+  return guard([&] {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    if (!h->x.ready) return FIP_OK;
+    ck(cudaStreamSynchronize(h->stream), "fip_exchange_wait");
+    ck(cudaStreamSynchronize(h->x.in), "fip_exchange_wait");
+    ck(cudaStreamSynchronize(h->x.out), "fip_exchange_wait");
+    h->x.out_pending[0] = h->x.out_pending[1] = false;
     return FIP_OK;
   });
 }

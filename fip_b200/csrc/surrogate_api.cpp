@@ -57,6 +57,8 @@ int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H,
   if (!x || !dy || !dw || N <= 0 || H <= 0 || W <= 0) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: bad argument");
   if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(dy)) & 15u)
     return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: tensors must be 16-byte aligned");
+  if ((long long)N * (H + 2 * fip::sg::kPad) * (W + 2 * fip::sg::kPad) >= (1LL << 31))
+    return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: too many pixels");
   if (dilation < 1 || dilation > fip::sg::kMaxDil) return sg_fail(FIP_ERR_ARG, "fip_sg_conv3x3_wgrad: dilation must be 1..8");
   int dev = 0;
   cudaGetDevice(&dev);

@@ -181,8 +181,8 @@ def fbm(W: int, H: int, hurst: float, seed: int) -> np.ndarray:
 def scenario1(outdir: str, W: int = 5667, H: int = 6500, dx: float = 3.0, dt: float = 0.5,
               duration: float = 3600.0 * 24, seed: int = 1, name: str = "scenario1",
               inflow_cells: int = 200, q_peak: float = 1500.0, t_peak: float = 6 * 3600.0,
-              q_end: float = 200.0, channel_width: int = 60, save_state: list | None = None
-              ) -> Scenario:
+              q_end: float = 200.0, channel_width: int = 60, save_state: list | None = None,
+              variable_dt: bool = True, wet_start: bool = False) -> Scenario:
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     scale = min(W, H) / 5667.0
@@ -242,15 +242,31 @@ def scenario1(outdir: str, W: int = 5667, H: int = 6500, dx: float = 3.0, dt: fl
     zpath = os.path.join(outdir, f"{name}_z.csv")
     write_series(qpath, ts, qs, header="time;discharge")
     write_series(zpath, ts, zs, header="time;stage")
+    init = {}
+    if wet_start:
+        # flooded start: water up to a level 1.5 m above the 35th terrain percentile (ponds and the
+        # channel), seeded discharges in the wet cells, dry on no_data cells
+        rng_w = np.random.default_rng(seed + 23)
+        level = float(np.percentile(z[~mask_nd], 35)) + 1.5
+        depth = np.clip(level - z, 0.0, 6.0).astype(np.float32)
+        depth[mask_nd] = 0.0
+        wet = depth > 0
+        qx0 = (0.3 * depth * rng_w.standard_normal((H, W)).astype(np.float32) * wet).astype(np.float32)
+        qy0 = (0.3 * depth * rng_w.standard_normal((H, W)).astype(np.float32) * wet).astype(np.float32)
+        for k, a in (("z", z + depth), ("qx", qx0), ("qy", qy0)):
+            path = os.path.join(outdir, f"{name}_{k}0.bin")
+            write_grid(path, a.astype(np.float32))
+            init[k] = [path, 0]
     cfg = {
-        "#0": f"seed {seed}: scenario1(W={W}, H={H}); inflow rows {r0}-{r1 - 1}",
+        "#0": f"seed {seed}: scenario1(W={W}, H={H}{', wet start' if wet_start else ''}); inflow rows {r0}-{r1 - 1}",
         "name": os.path.join(outdir, name),
         "terrain": [tpath, 16],
         "W": W, "H": H, "dx": dx, "dt": dt,
         "duration": "3600*24" if duration == 3600.0 * 24 else duration,
         "kSt_var": [kpath, 16],
+        **init,
         "no_data": no_data,
-        "variable_dt": True,
+        "variable_dt": variable_dt,
         "boundary_conditions": [
             {"side": "left", "type": "q", "q": [qpath, 0, 1], "z": [zpath, 0, 1],
              "from": r0, "to": r1 - 1},

@@ -47,7 +47,8 @@ typedef struct {
   int use_graphs;           /* run batches of steps as captured CUDA graphs (default 1) */
   int all_tiles;            /* compute every tile every step, no dry-tile skipping (default 0) */
   int stop_on_nonfinite;    /* fip_step/fip_run return FIP_ERR_NONFINITE at the first NaN/Inf depth */
-  int quiet;                /* write no sampling CSV (default 0: stdout, like the reference) */
+  int quiet;                /* write no sampling CSV and no loader warnings (default 0: stdout and
+                               stderr, like the reference; errors are always reported) */
   const char* sample_path;  /* write the sampling CSV to this file instead of stdout (NULL) */
 } fip_options;
 
@@ -110,6 +111,25 @@ int fip_get_field(fip_handle* h, int field, float* host_out);
  * buffer. No counterpart in the reference (which restarts only from files at start-up). */
 int fip_set_field(fip_handle* h, int field, const float* host_src);
 
+/* Pipelined state exchange with the host (no counterpart in the reference): for a host that
+ * replaces the whole state (h, qx, qy) from its own buffers, runs some steps and reads the state
+ * back, over and over, with inputs that do not depend on the previous outputs (restarts,
+ * replayed forcing). The host-device copies overlap the steps: the upload of the next state and
+ * the download of the last one run on two copy streams of the handle while the steps run.
+ *   fip_stage_state: queues the upload of a state (three W x H host grids; pinned memory lets the
+ *     copy run at the host link's speed) into one of two staging slots and returns at once. The
+ *     host buffers must stay unchanged until the fip_step_exchange that takes the state returns.
+ *     At most two states can wait (FIP_ERR_ARG beyond that).
+ *   fip_step_exchange: makes the oldest staged state (if any) the current state, exactly as
+ *     fip_set_field of the three fields does, runs n_steps steps (fip_step), and queues the
+ *     download of the resulting state into the three host buffers (all NULL: no download). It
+ *     returns once the steps are done; the downloads of a call are complete when the next call
+ *     returns or after fip_exchange_wait.
+ *   fip_exchange_wait: waits for every queued copy. */
+int fip_stage_state(fip_handle* h, const float* h_src, const float* qx_src, const float* qy_src);
+int fip_step_exchange(fip_handle* h, int n_steps, float* h_dst, float* qx_dst, float* qy_dst);
+int fip_exchange_wait(fip_handle* h);
+
 /* duration (s, FP64), dt of the next step, completed iterations (SimData::duration/dt/iteration). */
 int fip_time(fip_handle* h, double* duration, float* dt, int* iteration);
 
@@ -159,21 +179,23 @@ void fip_destroy(fip_handle* h);
 /* One rmg step of the whole grid on caller-owned device buffers, allocating nothing. No
  * counterpart in the reference. It is for callers that cannot allocate device memory: a host that
  * drives the step from its own time loop while other streams keep the GPU busy (cudaFree
- * synchronises the whole device), a host whose own pool owns all device memory, or code that
- * records the step into a CUDA graph.
+ * synchronises the whole device), or a host whose own memory pool owns all device memory and
+ * forbids allocations once it runs.
  * Inputs: h_in, qx_in, qy_in, terrain (and kst_or_null, else the uniform kst_fixed), pitched with
  * `pitch` elements per row (a multiple of 4), 16-byte aligned, W x H cells, W, H >= 4. Outputs:
  * h_out, qx_out, qy_out receive the step on the cells the reference's kernel writes; their other
  * cells are left as the caller set them (give them the input state, like the reference's
- * ping-pong partner). cfl_out_or_null (device float) receives the CFL minimum of the step (NaN if
- * a bounded device-side wait ran out). No boundary conditions, dt control or sampling: this is the
- * stencil alone (the launch of src/kernels.cu:441-455 with the mask off).
+ * ping-pong partner). cfl_out_or_null (device float) receives the CFL minimum of the step, or NaN
+ * if a bounded device-side wait ran out: a caller that must detect such a timeout passes it (with
+ * NULL a timed-out step still returns 0). No boundary conditions, dt control or sampling: this is
+ * the stencil alone (the launch of src/kernels.cu:441-455 with the mask off).
  * Scratch: a static device array sized for grids of at most 32768 tiles of 480 x 32 cells (about
  * 503 million cells); larger grids return FIP_ERR_ARG. Every GPU that loads the library holds
  * that array (about 160 KB) until the process exits. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress), so make that first call before any stream
- * capture. Calls share the array and overwrite what the step reads from it each time; calls that
- * overlap on the GPU (other streams or host threads) race on it. Runs on `stream` (a
+ * array's device address (cudaGetSymbolAddress) and keeps it for the life of the process, so
+ * make that first call before any stream capture, and do not reset the device (cudaDeviceReset)
+ * between calls. Calls share the array and rewrite what the step reads from it each time; calls
+ * that overlap on the GPU (other streams or host threads) race on it. Runs on `stream` (a
  * cudaStream_t, NULL for the legacy default stream) on the current device and returns without
  * synchronising. */
 int fip_rmg_step_noalloc(const float* h_in, const float* qx_in, const float* qy_in, const float* terrain,

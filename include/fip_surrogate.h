@@ -29,7 +29,10 @@ extern "C" {
 int fip_sg_conv3x3(const void* in, const void* w, const float* bias, const void* res, const void* mask, void* out,
                    int N, int H, int W, int dilation, int epi, int* dev_err, void* stream);
 
-/* dw (f32 [9][64 out][64 in]) = sum over pixels of x[p + tap offset][in] * dy[p][out]. */
+/* dw (f32 [9][64 out][64 in]) = sum over pixels of x[p + tap offset][in] * dy[p][out].
+ * The per-CTA partial sums go to one scratch buffer per device, allocated by the first call on
+ * that device and shared by every later call: wgrad calls on one device must not overlap (another
+ * stream or host thread), or they race on it. */
 int fip_sg_conv3x3_wgrad(const void* x, const void* dy, float* dw, int N, int H, int W, int dilation, int* dev_err,
                          void* stream);
 

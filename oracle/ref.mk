@@ -2,7 +2,7 @@
 # Test infrastructure only: the binaries are the parity pin for the CPU oracle and for the
 # CUDA solver. Nothing here is shipped or linked into the product.
 #
-#   make -f oracle/ref.mk REF=/root/reference        (run from the repository root)
+#   make -f oracle/ref.mk REF=<reference checkout>     (run from the repository root)
 #
 # Three binaries are produced, all from the reference's sources where they lie:
 #   _ref/fip_ref         as shipped (wet/dry mask on, host reads the CFL slots unsynchronised)
@@ -14,7 +14,10 @@
 # The patched copies are generated by sed at build time into _ref/patched/ (git-ignored); the
 # reference's own build system (CMake) is not used.
 
-REF      ?= /root/reference
+REF      ?= $(FIP_REFERENCE_SRC)
+ifeq ($(REF),)
+$(error set REF=<reference checkout> or FIP_REFERENCE_SRC)
+endif
 OUT      := oracle/_ref
 CUDA     ?= /usr/local/cuda
 NVCC     := $(CUDA)/bin/nvcc

@@ -98,3 +98,23 @@ def test_ensemble_all_tiles_matches(tmp_path):
         for m, p in enumerate(paths):
             ref, rt = _single(p, K)
             _check_member(e, m, ref, rt)
+
+
+@pytest.mark.parametrize("all_tiles,shape", [(True, (4, 32)), (False, (2, 16))])
+def test_large_ensemble_multi_chunk_members_match_single_runs(tmp_path, all_tiles, shape):
+    """Members of 0.5 to 3 M cells whose tiles together fill several 512-tile chunks of the
+    concatenated plan (1 131 tiles of 480 x 32, 3 957 of 240 x 16): every member still computes
+    exactly what its single run computes."""
+    sizes = [(2048, 1500), (1900, 1300), (1200, 2000), (2000, 900), (700, 1800), (1500, 1500), (1024, 1024)]
+    paths = [synth.ensemble_member(str(tmp_path), W, H, seed=40 + i, kst=22.0 + 3 * i, q_peak=800.0 + 150 * i,
+                                   t_peak=600.0, duration=3600.0, name=f"L{i}").yaml_path
+             for i, (W, H) in enumerate(sizes)]
+    K = 150
+    with Ensemble(paths, all_tiles=all_tiles) as e:
+        e.set_shape(*shape)
+        e.step(K)
+        inf = e.info()
+        assert inf.n_tiles > 1024
+        for m, p in enumerate(paths):
+            ref, rt = _single(p, K)
+            _check_member(e, m, ref, rt)

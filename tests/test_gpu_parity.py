@@ -239,3 +239,51 @@ def test_nonfinite_is_reported(tmp_path):
     assert e.value.code == -5
     assert sim.info().nonfinite == 1
     sim.close()
+
+
+def test_dry_tile_skipping_unconfigured_sides(tmp_path):
+    """Only the tiles a boundary condition writes near are always computed: sides without a
+    condition keep their edge cells as they are, so their dry tiles are skipped, while water lying
+    on edge cells the step never writes keeps the tiles within reach active. Runs with dry-tile
+    skipping stay bit-identical to every-tile runs."""
+    from fip_b200 import synth
+
+    W, H = 1500, 700
+    rng = np.random.default_rng(17)
+    y = np.arange(H, dtype=np.float32)[:, None]
+    x = np.arange(W, dtype=np.float32)[None, :]
+    terr = (0.002 * x + 0.3 * np.sin(x / 37.0) * np.cos(y / 23.0)).astype(np.float32)
+    depth = np.zeros((H, W), np.float32)
+    depth[250:420, 0:300] = 0.8                      # pond against the left side (z inflow rows 300-360)
+    depth[H - 3:H, 700:760] = 0.5                    # water on the top edge rows (never written there)
+    depth[100:140, W - 2:W] = 0.3                    # and on the right edge columns
+    depth[500:530, 900:960] = 0.6                    # an inland pond
+    wet = depth > 0
+    qx = (0.05 * rng.standard_normal((H, W)) * wet).astype(np.float32)
+    qy = (0.05 * rng.standard_normal((H, W)) * wet).astype(np.float32)
+    files = {}
+    for k, a in (("terrain", terr), ("z", terr + depth), ("qx", qx), ("qy", qy)):
+        files[k] = str(tmp_path / f"u_{k}.bin")
+        synth.write_grid(files[k], a)
+    cfg = {"name": str(tmp_path / "u"), "terrain": [files["terrain"], 0], "z": [files["z"], 0],
+           "qx": [files["qx"], 0], "qy": [files["qy"], 0], "W": W, "H": H, "dx": 2.0, "dt": 0.05,
+           "duration": 1000, "kSt": 30, "variable_dt": False,
+           "boundary_conditions": [{"side": "left", "type": "z", "z": float(terr[330, 0] + 1.2), "from": 300,
+                                    "to": 360}]}
+    path = str(tmp_path / "u.yml")
+    synth.write_yaml(path, cfg)
+    res = []
+    for all_tiles, graphs in ((True, False), (False, True), (False, False)):
+        sim = _sim(path, quiet=True, all_tiles=all_tiles, use_graphs=graphs)
+        first = sim.info().active_tiles
+        sim.step(300)
+        inf = sim.info()
+        res.append(({k: sim.field(k) for k, _ in FIELDS}, first, inf.active_tiles, inf.n_tiles))
+        sim.close()
+    ref = res[0][0]
+    for fields, first, active, n in res[1:]:
+        # 4 x 22 tiles, 48 of them on the edge: the dry edge tiles away from the water and from
+        # the inflow are skipped from the first step on
+        assert first < n and active < n, (first, active, n)
+        for k, _ in FIELDS:
+            assert np.array_equal(ref[k].view(np.uint32), fields[k].view(np.uint32)), k

@@ -105,6 +105,10 @@ def test_surrogate_entry_points_reject_bad_arguments():
     assert L.fip_sg_conv3x3(al, al, None, None, None, al, 1, 8, 8, 1, 7, None, None) == _lib.FIP_ERR_ARG  # epilogue
     assert L.fip_sg_conv3x3(al, al, None, None, None, al, 1, 8, 8, 1, 1, None, None) == _lib.FIP_ERR_ARG  # needs res
     assert L.fip_sg_conv3x3_wgrad(al, al, al, 1, 8, 8, 0, None, None) == _lib.FIP_ERR_ARG
+    big = (200, 3300, 3300)  # (3300 + 16)^2 * 200 pixels > 2^31
+    assert L.fip_sg_conv3x3(al, al, None, None, None, al, *big, 1, 0, None, None) == _lib.FIP_ERR_ARG
+    assert L.fip_sg_conv3x3_wgrad(al, al, al, *big, 1, None, None) == _lib.FIP_ERR_ARG
+    assert "too many pixels" in _lib.last_error()
     assert L.fip_sg_edges(al, al, 1, 8, 8, 0, 3, 1, 1, ctypes.c_float(-1.0), None) == _lib.FIP_ERR_ARG
     assert L.fip_sg_adamw(al, al, al, al, 10, ctypes.c_float(1e-3), ctypes.c_float(0.9), ctypes.c_float(0.999),
                           ctypes.c_float(1e-8), ctypes.c_float(0.0), 0, None) == _lib.FIP_ERR_ARG  # step >= 1
