@@ -207,6 +207,52 @@ def cpu_baseline(sc, seconds: float, steps_hint: int | None = None):
                       f"{n} steps in {dt:.1f} s, {threads} threads"}, n, dt
 
 
+def gpu_reference_baseline(args, local_rank, duration):
+    """Baseline leg: the reference's own CUDA kernels on this GPU. oracle/_ref holds the reference
+    built from its own sources (the parity pin of the tests; oracle/ref.mk): fip_ref_nomask computes
+    every strip (mask off), fip_ref skips dry strips with its wet/dry mask. Both run the large-grid
+    scenario for its first `duration` simulated seconds and report the reference's own timing line
+    (CUDA events around its whole simulate() loop, src/main.cpp:238-253). This library runs the same
+    parameter file through fip_run, timed around the loop (wall clock, the loop ends synchronised),
+    with every tile computed and with dry-tile skipping. Per-step time includes each side's host
+    work per step (the reference's host dt controller and launches; the graphs and device-side dt
+    control here)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refbin
+
+    from fip_b200 import Simulation, synth
+
+    d = os.path.join(tempfile.gettempdir(), f"fip_bench_ref_{os.getpid()}")
+    sc = synth.scenario1(d, W=args.W, H=args.H, seed=1, duration=duration, name="refcmp")
+    cells = sc.W * sc.H
+    out = {"workload": f"scenario1 {sc.W}x{sc.H}, variable dt, first {duration:g} simulated s (dry start)",
+           "source": "oracle/_ref binaries built from the reference's sources by oracle/ref.mk"}
+    for name, key in (("fip_ref_nomask", "reference_every_cell"), ("fip_ref", "reference_wet_dry_mask")):
+        if refbin.binary(name) is None:
+            out[key] = {"unavailable": f"oracle/_ref/{name} not built"}
+            continue
+        try:
+            r = refbin.run(name, sc.yaml_path, timeout=600)
+            out[key] = {"binary": f"oracle/_ref/{name}", "iterations": r["iterations"], "seconds": r["seconds"],
+                        "s_per_it": r["seconds"] / r["iterations"],
+                        "cell_updates_per_s": cells * r["iterations"] / r["seconds"]}
+        except Exception as exc:
+            out[key] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+    for all_tiles, key in ((True, "fip_b200_every_tile"), (False, "fip_b200_dry_skip")):
+        with Simulation(sc.yaml_path, device=local_rank, quiet=True, all_tiles=all_tiles) as sim:
+            t0 = time.perf_counter()
+            sim.run()
+            sec = time.perf_counter() - t0
+            it = sim.iteration
+        out[key] = {"iterations": it, "seconds": sec, "s_per_it": sec / it, "cell_updates_per_s": cells * it / sec}
+    a, b = out.get("reference_every_cell", {}), out.get("reference_wet_dry_mask", {})
+    if "s_per_it" in a:
+        out["speedup_every_cell"] = a["s_per_it"] / out["fip_b200_every_tile"]["s_per_it"]
+    if "s_per_it" in b:
+        out["speedup_dry_skip_vs_mask"] = b["s_per_it"] / out["fip_b200_dry_skip"]["s_per_it"]
+    return out
+
+
 def ensemble_measure(args, local_rank):
     """Batched ensemble of 64 scenarios (W, H ~ U[256, 2048], own fBm terrain, kSt ~ U[20, 45],
     triangular inflow peaking at U[200, 2000] m3/s after U[1, 8] h, variable dt), FP32.
@@ -427,6 +473,12 @@ def run_gpu(args, rank, world, local_rank):
             sgm = surrogate_measure(args)
         except Exception as exc:
             sgm = {"error": f"{type(exc).__name__}: {exc}"}
+    gref = None
+    if world == 1 and args.gpu_ref_seconds > 0:
+        try:
+            gref = gpu_reference_baseline(args, local_rank, args.gpu_ref_seconds)
+        except Exception as exc:
+            gref = {"error": f"{type(exc).__name__}: {exc}"[:300]}
     if rank == 0:
         base = None
         if world == 1 and not args.no_cpu_baseline:
@@ -442,7 +494,8 @@ def run_gpu(args, rank, world, local_rank):
                                 "steps + download into pinned host (fip_stage_state / fip_step_exchange: the "
                                 "copies of one e2e step overlap the solver steps of its neighbours)"},
                 "gpu_launches": 2 * args.steps, "roofline": roof, "clocks": clocks,
-                "cpu_baseline": base, "active_tiles": active, "ensemble": ens, "surrogate": sgm}
+                "cpu_baseline": base, "gpu_reference": gref, "active_tiles": active, "ensemble": ens,
+                "surrogate": sgm}
         print(json.dumps(line), flush=True)
     replicas.finish(dist)
     return 0
@@ -461,6 +514,8 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=8, help="e2e steps (at least; more when --steps is larger)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gpu-ref-seconds", type=float, default=120.0,
+                    help="simulated s of the reference-binary baseline on this GPU (0: skip)")
     ap.add_argument("--ens-members", type=int, default=64, help="batched-ensemble measurement (0: skip)")
     ap.add_argument("--ens-steps", type=int, default=200)
     ap.add_argument("--ens-seq-steps", type=int, default=20)

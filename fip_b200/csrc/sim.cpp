@@ -26,6 +26,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "bc_codegen.h"
 #include "config.h"
 #include "drv.h"
@@ -61,6 +63,15 @@ constexpr double kInf = std::numeric_limits<double>::infinity();
 namespace fip {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace fip
+
+namespace {
+// NVTX range for the lifetime of a scope (visible under Nsight Systems / ncu --nvtx; a no-op when
+// no tool is attached)
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+};
+}  // namespace
 
 struct fip_handle {
   fip::Config cfg;
@@ -422,6 +433,7 @@ void fip_handle::flush_hmax_if_due() {
 
 void fip_handle::sample() {  // sample (src/main.cpp:53-83)
   if (!out) return;
+  Range range("sampling");
   const int np = (int)cfg.points.size();
   if (np) {
     ck(fip::launch_sample_gather(st, h_ctl->parity, np, d_sample_idx, d_sample_val, stream), "sample");
@@ -435,6 +447,7 @@ void fip_handle::sample() {  // sample (src/main.cpp:53-83)
 
 void fip_handle::dump(const std::string& prefix, bool current) {
   // dumpDeviceBuffers (src/main.cpp:180-202)
+  Range range("save_state dump");
   ck(cudaStreamSynchronize(stream), "dump");
   const size_t W = cfg.W, H = cfg.H;
   std::vector<float> buf(W * H);
@@ -461,6 +474,7 @@ void fip_handle::dump(const std::string& prefix, bool current) {
 
 // Runs up to `budget` simulate() calls (or until target_duration when to_target).
 int fip_handle::run_steps(long long budget, bool to_target) {
+  Range range("fip steps");
   ck(cudaSetDevice(device), "cudaSetDevice");
   if (to_target && h_ctl->duration >= cfg.target_duration) return FIP_OK;
   if (budget <= 0) return FIP_OK;
@@ -475,10 +489,12 @@ int fip_handle::run_steps(long long budget, bool to_target) {
     h_ctl->stop_reason = 0;
     h_ctl->steps_left = 1;
     write_ctl_fields();
+    Range r0("boundary conditions, iteration 0");
     launch_post(FIP_POST_MODE_INIT);
     started = true;
   }
   if (replan) {
+    Range r1("active-tile plan");
     ck(fip::launch_init_tiles(st, h_ctl->parity, stream), "init_tiles");
     launch_post(FIP_POST_MODE_PLAN);
     replan = false;
@@ -491,8 +507,11 @@ int fip_handle::run_steps(long long budget, bool to_target) {
   const int it0 = h_ctl->iteration;
   int rc = FIP_OK;
   for (;;) {
-    launch_batch(steps_hint());
-    read_ctl();
+    {
+      Range rb("batch: stencil + boundary conditions / plan / dt");
+      launch_batch(steps_hint());
+      read_ctl();
+    }
     if (h_ctl->error) return fail(FIP_ERR_DEVICE_TIMEOUT, "device wait ran out (code " + std::to_string(h_ctl->error) + ")");
     const int reason = h_ctl->stop ? h_ctl->stop_reason : 0;
     bool done = false;
@@ -787,6 +806,7 @@ int fip_volume(fip_handle* h, double* outv) {
   if (!h || !outv) return fail(FIP_ERR_ARG, "null argument");
   return guard([&] {
     ck(cudaSetDevice(h->device), "cudaSetDevice");
+    Range range("volume reduction (FP64)");
     ck(fip::launch_volume(h->st, h->h_ctl->parity, h->d_vol_partials, h->d_vol, h->stream), "volume");
     double v = 0;
     ck(cudaMemcpyAsync(&v, h->d_vol, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "volume");
