@@ -501,6 +501,31 @@ def run_gpu(args, rank, world, local_rank):
     return 0
 
 
+def time_to_solution(args):
+    """The large-grid scenario over its whole duration (24 simulated hours, variable dt, dry-tile
+    skipping) through fip_run, and optionally the reference binary (wet/dry mask on) on the same
+    parameter file: wall seconds and steps. Prints one JSON object (not a bench line)."""
+    from fip_b200 import Simulation, synth
+
+    d = os.path.join(tempfile.gettempdir(), f"fip_tts_{os.getpid()}")
+    sc = synth.scenario1(d, W=args.W, H=args.H, seed=1, duration=args.tts_hours * 3600.0, name="tts")
+    out = {"workload": f"scenario1 {sc.W}x{sc.H}, {args.tts_hours:g} simulated hours, variable dt"}
+    with Simulation(sc.yaml_path, quiet=True) as sim:
+        t0 = time.perf_counter()
+        sim.run()
+        out["fip_b200"] = {"wall_s": time.perf_counter() - t0, "steps": sim.iteration,
+                           "final_dt": sim.time()[1], "active_tile_fraction_end": sim.info().active_tiles / sim.info().n_tiles}
+    if args.tts_reference:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import refbin
+
+        r = refbin.run("fip_ref", sc.yaml_path, timeout=7200)
+        out["reference_fip_ref"] = {"seconds": r["seconds"], "steps": r["iterations"]}
+        out["speedup"] = r["seconds"] / out["fip_b200"]["wall_s"]
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -525,7 +550,12 @@ def main():
     ap.add_argument("--sg-hours", type=float, default=0.5)
     ap.add_argument("--sg-steps", type=int, default=300)
     ap.add_argument("--sg-batch", type=int, default=16)
+    ap.add_argument("--tts", action="store_true", help="only the time-to-solution run of the large grid")
+    ap.add_argument("--tts-hours", type=float, default=24.0)
+    ap.add_argument("--tts-reference", action="store_true", help="also run the reference binary for --tts")
     args = ap.parse_args()
+    if args.tts:
+        return time_to_solution(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

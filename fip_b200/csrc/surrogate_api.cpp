@@ -133,6 +133,13 @@ int fip_sg_apply(const float* pred, int N, int H, int W, float dx, const float* 
   return sg_cuda(fip::sg::apply_update(pred, N, H, W, dx, terrain, no_value, h, qx, qy, dvol, hmax, SG_S), "fip_sg_apply");
 }
 
+int fip_sg_consistency(const float* pred, int N, int H, int W, float dx, const float* terrain, float no_value,
+                       const float* qx, const float* qy, double* res, void* stream) {
+  if (!pred || !terrain || !qx || !qy || !res || N <= 0 || (long long)H * W < 256 || H < 3 || W < 4 || !(dx > 0.f))
+    return sg_fail(FIP_ERR_ARG, "fip_sg_consistency: bad argument (images of at least 256 cells)");
+  return sg_cuda(fip::sg::consistency(pred, N, H, W, dx, terrain, no_value, qx, qy, res, SG_S), "fip_sg_consistency");
+}
+
 int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, void* stream) {
   if (!qx || !qy || !flux || N <= 0 || H < 3 || W < 3) return sg_fail(FIP_ERR_ARG, "fip_sg_edge_flux: bad argument");
   return sg_cuda(fip::sg::edge_flux(qx, qy, N, H, W, flux, SG_S), "fip_sg_edge_flux");

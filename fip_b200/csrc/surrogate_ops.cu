@@ -229,6 +229,58 @@ __global__ void apply_kernel(const float* __restrict__ pred, int N, int H, int W
   }
 }
 
+// Consistency residual of one call, before the update: the network predicts the water moved
+// through each face twice, as the mean face discharges (Fx, Fy: the depth change by continuity)
+// and as the change of the discharges (dqx, dqy: the mean discharge over the call by the
+// trapezoid rule, q + dq / 2). Per inner cell the depth changes they imply differ by
+// |dh_F - dh_q|; res[n] += the sum over image n (a depth sum: times dx^2 a volume). A network that
+// left the states it was trained on stops agreeing with itself.
+__global__ void consistency_kernel(const float* __restrict__ pred, int N, int H, int W, float c,
+                                   const float* __restrict__ terr, float no_value, const float* __restrict__ qx,
+                                   const float* __restrict__ qy, double* __restrict__ res) {
+  __shared__ double red[2][256];
+  __shared__ int s_n0;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t total = (size_t)N * H * W;
+  const size_t img = (size_t)H * W;
+  double r = 0.0;
+  int n = 0;
+  if (i < total) {
+    n = (int)(i / img);
+    const int y = (int)((i / W) % H), x = (int)(i % W);
+    const bool inner = x >= 2 && x <= W - 2 && y >= 1 && y <= H - 2;
+    if (inner && terr[i] != no_value) {
+      const size_t p = ppix(n, y, x, H, W);
+      const int Wp = W + 2 * kPad;
+      const float dhf = dh_of(pred, p, Wp, c);
+      // mean discharges of the faces east / west / north / south of the cell over the call
+      const float fe = qx[i] + 0.5f * kOutQ * pred[p * 4 + 2];
+      const float fw = qx[i - 1] + 0.5f * kOutQ * pred[(p - 1) * 4 + 2];
+      const float fn = qy[i] + 0.5f * kOutQ * pred[p * 4 + 3];
+      const float fs = qy[i - W] + 0.5f * kOutQ * pred[(p - Wp) * 4 + 3];
+      const float dhq = -(c / kOutF) * ((fe - fw) + (fn - fs));
+      r = fabs((double)dhf - (double)dhq);
+    }
+  }
+  if (threadIdx.x == 0) s_n0 = (int)(((size_t)blockIdx.x * blockDim.x) / img);
+  __syncthreads();
+  const int slot = n - s_n0;
+  red[0][threadIdx.x] = (i < total && slot == 0) ? r : 0.0;
+  red[1][threadIdx.x] = (i < total && slot == 1) ? r : 0.0;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + s];
+      red[1][threadIdx.x] += red[1][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(&res[s_n0], red[0][0]);
+    if (s_n0 + 1 < N && red[1][0] != 0.0) atomicAdd(&res[s_n0 + 1], red[1][0]);
+  }
+}
+
 // Net discharge into the inner cells [2, W-2] x [1, H-2] per image (qx sits on east faces,
 // qy on north faces): + qx[y][1] - qx[y][W-2] over rows 1..H-2, + qy[0][x] - qy[H-2][x] over
 // columns 2..W-2 (a sum of discharges per unit width; times dx gives m3/s).
@@ -354,6 +406,14 @@ cudaError_t apply_update(const float* pred, int N, int H, int W, float dx, const
   const size_t total = (size_t)N * H * W;
   apply_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(pred, N, H, W, kCallS / dx * kOutF, terr, no_value, h,
                                                                 qx, qy, dvol, hmax);
+  return cudaGetLastError();
+}
+
+cudaError_t consistency(const float* pred, int N, int H, int W, float dx, const float* terr, float no_value,
+                        const float* qx, const float* qy, double* res, cudaStream_t s) {
+  const size_t total = (size_t)N * H * W;
+  consistency_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(pred, N, H, W, kCallS / dx * kOutF, terr,
+                                                                      no_value, qx, qy, res);
   return cudaGetLastError();
 }
 

@@ -197,14 +197,19 @@ class Surrogate:
         self.cast()
 
     # ---- one surrogate call ------------------------------------------------------------------
-    def advance(self, state, pins=None, hmax=None):
+    def advance(self, state, pins=None, hmax=None, resid=None):
         """state: dict of device tensors h, qx, qy, terrain, kst [N][H][W], zref [N], no_value;
-        h/qx/qy advance by 60 s in place (hmax, if given, folds the new depths). Returns the
+        h/qx/qy advance by 60 s in place (hmax, if given, folds the new depths; resid, a device
+        double [N], accumulates the call's consistency residual, fip_sg_consistency). Returns the
         per-image depth-sum change of the inner cells (device double [N])."""
         h, qx, qy = state["h"], state["qx"], state["qy"]
         N, H, W = h.shape
         self.pack(h, qx, qy, state["terrain"], state["kst"], state["zref"], state["no_value"], N, H, W)
         pred = self.forward(N, H, W)
+        if resid is not None:
+            _lib.check(self.L.fip_sg_consistency(_ptr(pred), N, H, W, float(state.get("dx", 3.0)),
+                                                 _ptr(state["terrain"]), float(state["no_value"]), _ptr(qx),
+                                                 _ptr(qy), _ptr(resid), _stream()))
         dvol = self.torch.zeros(N, dtype=self.torch.float64, device=self.dev)
         _lib.check(self.L.fip_sg_apply(_ptr(pred), N, H, W, float(state.get("dx", 3.0)), _ptr(state["terrain"]),
                                        float(state["no_value"]), _ptr(h), _ptr(qx), _ptr(qy), _ptr(dvol),

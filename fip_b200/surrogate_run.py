@@ -218,33 +218,105 @@ def evaluate_one_call(net: Surrogate, batch: Batch, snaps):
 
 def rollout(net: Surrogate, batch: Batch, n_calls: int, h0, qx0, qy0, residual_threshold: float = 1e-3):
     """Closed-loop surrogate run from (h0, qx0, qy0) over n_calls calls: final state, max-depth
-    maps (over the 60-s states) and, per member, whether the mass-balance residual tripped:
-    |change of inner volume - 60 s x mean edge inflow| > threshold x inner volume, checked at
-    every call (inner cells [2, W-2] x [1, H-2]: the left z condition also sets column 1)."""
+    maps (over the 60-s states) and, per member, whether the fallback indicator tripped and its
+    worst value. The indicator of a call is the network's consistency residual (fip_sg_consistency:
+    the volume on which its face-discharge and discharge-change outputs disagree) relative to the
+    member's water volume (inner cells, floor 1 cm over 1 % of them); it trips above
+    `residual_threshold` (1e-3 of the patch volume) at any call. The mass-balance residual of
+    the state (change of inner volume against 60 s x the mean edge inflow) is reported beside it."""
     torch = _torch()
     st = {"h": h0.clone(), "qx": qx0.clone(), "qy": qy0.clone()}
     state = batch.state(st["h"], st["qx"], st["qy"])
     net.pin(state, batch.pins)  # the iteration-0 boundary conditions
     hmax = st["h"].clone()
-    tripped = np.zeros(batch.n, bool)
     worst = np.zeros(batch.n)
+    worst_mass = np.zeros(batch.n)
     dx = 3.0
     h_host = st["h"].cpu().numpy()
     vol = h_host[:, 1:-1, 2:-1].astype(np.float64).sum(axis=(1, 2))
-    # floor of the reference volume: 1 cm of water over 1 % of the inner cells (a dry start
-    # would otherwise make every relative residual infinite)
     floor = 0.01 * 0.01 * (batch.H - 2) * (batch.W - 3)
+    resid = torch.zeros(batch.n, dtype=torch.float64, device=net.dev)
     for c in range(n_calls):
         f0 = net.edge_flux(st["qx"], st["qy"])
-        dvol = net.advance(state, batch.pins, hmax)
+        resid.zero_()
+        dvol = net.advance(state, batch.pins, hmax, resid=resid)
         f1 = net.edge_flux(st["qx"], st["qy"])
-        dv, a, b = dvol.cpu().numpy(), f0.cpu().numpy(), f1.cpu().numpy()
+        dv, a, b, r = dvol.cpu().numpy(), f0.cpu().numpy(), f1.cpu().numpy(), resid.cpu().numpy()
         vol = vol + dv
-        rel = np.abs(dv - CALL_S / dx * 0.5 * (a + b)) / np.maximum(vol, floor)
-        worst = np.maximum(worst, rel)
-        tripped |= rel > residual_threshold
+        denom = np.maximum(vol, floor)
+        worst = np.maximum(worst, r / denom)
+        worst_mass = np.maximum(worst_mass, np.abs(dv - CALL_S / dx * 0.5 * (a + b)) / denom)
     torch.cuda.synchronize()
-    return st, hmax, tripped, worst
+    tripped = worst > residual_threshold
+    return st, hmax, tripped, worst, worst_mass
+
+
+def screen(net: Surrogate, sc, hours: float, chunk: int = 32, top_frac: float = 0.1, threshold: float = 1e-3):
+    """Surrogate-screened ensemble: every member rolled out by the surrogate (chunks of `chunk`
+    members) to max-depth maps; the most flooded `top_frac` and every member whose fallback
+    indicator tripped are re-run by the batched solver. Judged against the batched solver on
+    every member: max-depth RMSE, flooded-extent IoU at 5 cm, wall times."""
+    torch = _torch()
+    n_sc = int(round(hours * 3600 / CALL_S))
+    n = len(sc)
+    H, W = sc[0].H, sc[0].W
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ref_hmax = torch.empty((n, H, W), dtype=torch.float32, device="cuda")
+    with Ensemble([s.yaml_path for s in sc]) as e:
+        e.step(n_sc * STEPS_PER_CALL)
+        e.gather("hmax", ref_hmax)
+    torch.cuda.synchronize()
+    t_solver_all = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    s_hmax = torch.empty_like(ref_hmax)
+    tripped = np.zeros(n, bool)
+    worst = np.zeros(n)
+    worst_mass = np.zeros(n)
+    for c0 in range(0, n, chunk):
+        part = sc[c0:c0 + chunk]
+        bsc = Batch(part)
+        h0 = torch.zeros((bsc.n, H, W), dtype=torch.float32, device="cuda")
+        q0 = torch.zeros_like(h0)
+        _, hm, tr, wo, wm = rollout(net, bsc, n_sc, h0, q0, q0.clone(), residual_threshold=threshold)
+        s_hmax[c0:c0 + bsc.n].copy_(hm)
+        tripped[c0:c0 + bsc.n], worst[c0:c0 + bsc.n], worst_mass[c0:c0 + bsc.n] = tr, wo, wm
+        del bsc, hm
+    t_surrogate = time.perf_counter() - t0
+    area = (s_hmax.cpu().numpy() > 0.05).sum(axis=(1, 2))
+    k = max(1, int(round(top_frac * n)))
+    rerun = sorted(set(np.argsort(-area)[:k].tolist()) | set(np.nonzero(tripped)[0].tolist()))
+    final = s_hmax.clone()
+    t0 = time.perf_counter()
+    if rerun:
+        with Ensemble([sc[i].yaml_path for i in rerun]) as e:
+            e.step(n_sc * STEPS_PER_CALL)
+            rh = torch.empty((len(rerun), H, W), dtype=torch.float32, device="cuda")
+            e.gather("hmax", rh)
+        for j, i in enumerate(rerun):
+            final[i].copy_(rh[j])
+    torch.cuda.synchronize()
+    t_rerun = time.perf_counter() - t0
+    fin, ref, sur = final.cpu().numpy(), ref_hmax.cpu().numpy(), s_hmax.cpu().numpy()
+    t_screen = t_surrogate + t_rerun
+    return {"members": n, "size": [H, W], "hours": hours, "rerun": len(rerun), "top_fraction": top_frac,
+            "fallback_tripped": int(tripped.sum()), "fallback_threshold": threshold,
+            "indicator_median": float(np.median(worst)), "indicator_max": float(np.max(worst)),
+            "mass_balance_residual_median": float(np.median(worst_mass)),
+            "wall_s_screened": round(t_screen, 2), "wall_s_surrogate": round(t_surrogate, 2),
+            "wall_s_rerun": round(t_rerun, 2), "wall_s_batched_solver_all": round(t_solver_all, 2),
+            "speedup": round(t_solver_all / max(t_screen, 1e-9), 3),
+            "rmse_hmax_m": _rmse(fin, ref), "iou_5cm": float(np.mean([_iou(fin[i], ref[i]) for i in range(n)])),
+            "rmse_hmax_surrogate_only_m": _rmse(sur, ref),
+            "iou_5cm_surrogate_only": float(np.mean([_iou(sur[i], ref[i]) for i in range(n)])),
+            "indicator_vs_error_spearman": _spearman(worst, np.sqrt(((sur - ref) ** 2).mean(axis=(1, 2))))}
+
+
+def _spearman(a, b):
+    ra, rb = np.argsort(np.argsort(a)), np.argsort(np.argsort(b))
+    if np.std(ra) == 0 or np.std(rb) == 0:
+        return 0.0
+    return float(np.corrcoef(ra, rb)[0, 1])
 
 
 def main(argv=None, emit: bool = True):
@@ -261,81 +333,63 @@ def main(argv=None, emit: bool = True):
     ap.add_argument("--screen-members", type=int, default=32)
     ap.add_argument("--screen-size", type=int, default=512)
     ap.add_argument("--screen-hours", type=float, default=1.0)
-    ap.add_argument("--out", default="")
+    ap.add_argument("--screen-chunk", type=int, default=32, help="members per surrogate rollout batch")
+    ap.add_argument("--threshold", type=float, default=1e-3, help="fallback: consistency residual / patch volume")
+    ap.add_argument("--params", default="", help="trained parameters (.npy): skip data generation and training")
+    ap.add_argument("--no-eval", action="store_true", help="skip the held-out evaluation")
+    ap.add_argument("--out", default="", help="write the trained parameters (.npy) here")
     a = ap.parse_args(argv)
     torch = _torch()
     d = tempfile.mkdtemp(prefix="fip_sg_")
     n_calls = int(round(a.hours * 3600 / CALL_S))
     res = {"config": vars(a)}
-    # ---- training data from the solver
-    tr = config3_members(d, a.members, a.size, seed=1, duration=a.hours * 3600 + 600)
-    btr = Batch(tr)
-    snaps, _, t_gen = solver_trajectories(tr, n_calls)
-    res["train_data"] = {"pairs": a.members * n_calls, "solver_s": round(t_gen, 2)}
-    # ---- training
-    net = Surrogate(seed=0)
-    log, t_train = train(net, btr, snaps, a.steps, bs=a.batch, lr=a.lr, pushforward=a.pushforward, unroll=a.unroll)
-    res["train"] = {"loss_log": log, "seconds": round(t_train, 2), "steps": a.steps,
-                    "ms_per_step": round(1e3 * t_train / max(a.steps, 1), 2)}
-    del snaps
-    torch.cuda.empty_cache()
-    # ---- held-out evaluation
-    ev = config3_members(d, a.eval_members, a.size, seed=2, duration=a.hours * 3600 + 600)
-    bev = Batch(ev)
-    esn, ehmax, _ = solver_trajectories(ev, n_calls)
-    res["eval_one_call"] = evaluate_one_call(net, bev, esn)
-    res["eval_trace"] = rollout_trace(net, bev, esn)
-    st, hm, tripped, worst = rollout(net, bev, n_calls, esn["h"][0], esn["qx"][0], esn["qy"][0])
-    ref_h = esn["h"][n_calls].cpu().numpy()
-    got_h = st["h"].cpu().numpy()
-    pers = esn["h"][0].cpu().numpy()
-    res["eval_rollout"] = {"calls": n_calls, "rmse_final_depth_m": _rmse(got_h, ref_h),
-                           "rmse_final_depth_persistence_m": _rmse(pers, ref_h),
-                           "rmse_hmax_m": _rmse(hm.cpu().numpy(), ehmax.cpu().numpy()),
-                           "iou_hmax_5cm": float(np.mean([_iou(hm[i].cpu().numpy(), ehmax[i].cpu().numpy())
-                                                          for i in range(bev.n)])),
-                           "fallback_tripped": int(tripped.sum()), "worst_residual": float(np.max(worst))}
-    del esn
-    torch.cuda.empty_cache()
+    if a.params:
+        net = Surrogate(params=np.load(a.params))
+        res["train"] = {"params": a.params}
+    else:
+        # ---- training data from the solver
+        tr = config3_members(d, a.members, a.size, seed=1, duration=a.hours * 3600 + 600)
+        btr = Batch(tr)
+        snaps, _, t_gen = solver_trajectories(tr, n_calls)
+        res["train_data"] = {"pairs": a.members * n_calls, "solver_s": round(t_gen, 2)}
+        # ---- training
+        net = Surrogate(seed=0)
+        log, t_train = train(net, btr, snaps, a.steps, bs=a.batch, lr=a.lr, pushforward=a.pushforward,
+                             unroll=a.unroll)
+        res["train"] = {"loss_log": log, "seconds": round(t_train, 2), "steps": a.steps,
+                        "ms_per_step": round(1e3 * t_train / max(a.steps, 1), 2)}
+        del snaps, btr
+        torch.cuda.empty_cache()
+        if a.out:
+            np.save(a.out, net.params())
+    if not a.no_eval:
+        # ---- held-out evaluation
+        ev = config3_members(d, a.eval_members, a.size, seed=2, duration=a.hours * 3600 + 600)
+        bev = Batch(ev)
+        esn, ehmax, _ = solver_trajectories(ev, n_calls)
+        res["eval_one_call"] = evaluate_one_call(net, bev, esn)
+        res["eval_trace"] = rollout_trace(net, bev, esn)
+        st, hm, tripped, worst, worst_mass = rollout(net, bev, n_calls, esn["h"][0], esn["qx"][0], esn["qy"][0],
+                                                     residual_threshold=a.threshold)
+        ref_h = esn["h"][n_calls].cpu().numpy()
+        got_h = st["h"].cpu().numpy()
+        pers = esn["h"][0].cpu().numpy()
+        ehm = ehmax.cpu().numpy()
+        hmn = hm.cpu().numpy()
+        err = np.sqrt(((hmn - ehm) ** 2).mean(axis=(1, 2)))
+        res["eval_rollout"] = {"calls": n_calls, "rmse_final_depth_m": _rmse(got_h, ref_h),
+                               "rmse_final_depth_persistence_m": _rmse(pers, ref_h),
+                               "rmse_hmax_m": _rmse(hmn, ehm),
+                               "iou_hmax_5cm": float(np.mean([_iou(hmn[i], ehm[i]) for i in range(bev.n)])),
+                               "fallback_tripped": int(tripped.sum()), "indicator": worst.tolist(),
+                               "hmax_rmse_per_member_m": err.tolist(),
+                               "indicator_vs_error_spearman": _spearman(worst, err),
+                               "mass_balance_residual": worst_mass.tolist()}
+        del esn
+        torch.cuda.empty_cache()
     # ---- screening
-    n_sc = int(round(a.screen_hours * 3600 / CALL_S))
     sc = config3_members(d, a.screen_members, a.screen_size, seed=3, duration=a.screen_hours * 3600)
-    bsc = Batch(sc)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    with Ensemble([s.yaml_path for s in sc]) as e:
-        e.step(n_sc * STEPS_PER_CALL)
-        ref_hmax = torch.empty((bsc.n, bsc.H, bsc.W), dtype=torch.float32, device="cuda")
-        e.gather("hmax", ref_hmax)
-    torch.cuda.synchronize()
-    t_solver_all = time.perf_counter() - t0
-    h0 = torch.zeros((bsc.n, bsc.H, bsc.W), dtype=torch.float32, device="cuda")
-    q0 = torch.zeros_like(h0)
-    t0 = time.perf_counter()
-    _, s_hmax, tripped, worst = rollout(net, bsc, n_sc, h0, q0, q0.clone())
-    area = (s_hmax.cpu().numpy() > 0.05).sum(axis=(1, 2))
-    k = max(1, int(round(0.1 * bsc.n)))
-    rerun = set(np.argsort(-area)[:k].tolist()) | set(np.nonzero(tripped)[0].tolist())
-    rerun = sorted(rerun)
-    final = s_hmax.clone()
-    if rerun:
-        with Ensemble([sc[i].yaml_path for i in rerun]) as e:
-            e.step(n_sc * STEPS_PER_CALL)
-            rh = torch.empty((len(rerun), bsc.H, bsc.W), dtype=torch.float32, device="cuda")
-            e.gather("hmax", rh)
-        for j, i in enumerate(rerun):
-            final[i].copy_(rh[j])
-    torch.cuda.synchronize()
-    t_screen = time.perf_counter() - t0
-    fin, ref = final.cpu().numpy(), ref_hmax.cpu().numpy()
-    res["screening"] = {"members": bsc.n, "size": bsc.H, "hours": a.screen_hours, "rerun": len(rerun),
-                        "fallback_tripped": int(tripped.sum()), "wall_s_screened": round(t_screen, 2),
-                        "wall_s_batched_solver_all": round(t_solver_all, 2),
-                        "speedup": round(t_solver_all / max(t_screen, 1e-9), 3),
-                        "rmse_hmax_m": _rmse(fin, ref), "iou_5cm": float(np.mean([_iou(fin[i], ref[i]) for i in range(bsc.n)])),
-                        "rmse_hmax_surrogate_only_m": _rmse(s_hmax.cpu().numpy(), ref)}
-    if a.out:
-        np.save(a.out, net.params())
+    res["screening"] = screen(net, sc, a.screen_hours, chunk=a.screen_chunk, threshold=a.threshold)
     if emit:
         print(json.dumps(res), flush=True)
     return res

@@ -70,6 +70,12 @@ int fip_sg_cast_weights(const float* p, int n_layers, void* wf, void* wd, void* 
  * (H * W >= 256); hmax (may be NULL) = max(hmax, new h). */
 int fip_sg_apply(const float* pred, int N, int H, int W, float dx, const float* terrain, float no_value, float* h,
                  float* qx, float* qy, double* dvol, float* hmax, void* stream);
+/* Fallback indicator of one call, evaluated before fip_sg_apply: res[n] += sum over the inner
+ * cells of image n (H * W >= 256) of |dh_F - dh_q|, the disagreement between the depth change
+ * the face-discharge outputs imply (continuity) and the one the discharge-change outputs imply
+ * (mean discharge over the call, q + dq / 2). A depth sum: times dx^2 it is a volume. */
+int fip_sg_consistency(const float* pred, int N, int H, int W, float dx, const float* terrain, float no_value,
+                       const float* qx, const float* qy, double* res, void* stream);
 /* flux[n] = net discharge per unit width into the inner cells [2, W-2] x [1, H-2] of image n
  * (through qx[:, 1], qx[:, W-2], qy[0, :], qy[H-2, :]). */
 int fip_sg_edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, void* stream);

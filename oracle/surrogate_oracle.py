@@ -89,3 +89,21 @@ def loss_and_grads(p, x, target, dx=3.0):
         g = (conv_oracle.conv3x3(dh, conv_oracle.dgrad_weights(w1), DIL[1 + 2 * k]) + g) * (acts[f"a{k}"] > 0)
     put(0, x, g)
     return loss, grads, pred
+
+
+def consistency(pred, qx, qy, terrain, no_value, dx=3.0):
+    """Fallback indicator of one call (fip_sg_consistency): per image, the sum over the inner cells
+    [2, W-2] x [1, H-2] (not no_data) of |dh_F - dh_q|, dh_F from the face discharges (continuity)
+    and dh_q from the mean discharges q + dq / 2 of the four faces. pred: [N, H, W, 4]."""
+    c = 60.0 / dx
+    dhf = depth_change(pred.astype(np.float64), dx)
+    fx = qx.astype(np.float64) + 0.5 * pred[..., 2]
+    fy = qy.astype(np.float64) + 0.5 * pred[..., 3]
+    fxw = np.pad(fx, ((0, 0), (0, 0), (1, 0)))[:, :, :-1]
+    fys = np.pad(fy, ((0, 0), (1, 0), (0, 0)))[:, :-1, :]
+    dhq = -c * (fx - fxw + fy - fys)
+    N, H, W = qx.shape
+    inner = np.zeros((H, W), bool)
+    inner[1:H - 1, 2:W - 1] = True
+    m = inner[None] & (terrain != no_value)
+    return np.array([np.abs(dhf[n] - dhq[n])[m[n]].sum() for n in range(N)])

@@ -89,3 +89,30 @@ def test_training_reduces_loss():
             losses.append(float(net.loss_acc.item()) / tgt.size)
     net.check_device()
     assert losses[-1] < 0.2 * losses[0], losses
+
+
+def test_consistency_indicator_matches_oracle():
+    """fip_sg_consistency (the fallback indicator) against its FP64 restatement."""
+    import ctypes
+
+    from fip_b200 import _lib
+
+    N, H, W = 3, 37, 29
+    rng = np.random.default_rng(11)
+    pred = (rng.standard_normal((N, H + 16, W + 16, 4)) * 0.3).astype(np.float32)
+    pred[:, :8] = pred[:, -8:] = 0.0  # the network output's zero border
+    pred[:, :, :8] = pred[:, :, -8:] = 0.0
+    qx = (rng.standard_normal((N, H, W)) * 0.5).astype(np.float32)
+    qy = (rng.standard_normal((N, H, W)) * 0.5).astype(np.float32)
+    terr = rng.standard_normal((N, H, W)).astype(np.float32)
+    terr[1, 10:13, 5:9] = -9999.0
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    res = torch.zeros(N, dtype=torch.float64, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    tp, tq, tr, tt = dev(pred), dev(qx), dev(qy), dev(terr)
+    rc = _lib.lib().fip_sg_consistency(p(tp), N, H, W, 3.0, p(tt), -9999.0, p(tq), p(tr), p(res),
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, _lib.last_error()
+    ref = so.consistency(pred[:, 8:-8, 8:-8].astype(np.float64), qx, qy, terr, -9999.0)
+    got = res.cpu().numpy()
+    assert np.allclose(got, ref, rtol=1e-5), (got, ref)
