@@ -46,10 +46,14 @@ constexpr int kNSlotMax = 10;  // ring depth in rows: 6 with the kSt field, else
 constexpr int kNSlotKvar2 = 8;
 constexpr int kNSlotUniform2 = 10;
 constexpr int kMinCtas2 = 5;
-constexpr int kMinCtas = 3;  // resident CTAs per SM (128 registers per thread)
-constexpr int kFieldBytes = FIP_SMEM_COLS * 4;  // 2048 B per staged row of one field
-constexpr int kConsumerWarps = 4;
-constexpr int kThreads = (kConsumerWarps + 1) * 32;
+constexpr int kMinCtas4 = 3;  // resident CTAs per SM (128 registers per thread)
+// narrow threads (2 columns each, tiles of 240 columns): half the registers, more CTAs per SM
+#ifndef FIP_NARROW_CTAS
+#define FIP_NARROW_CTAS 4
+#endif
+constexpr int kMinCtasNarrow = FIP_NARROW_CTAS;
+constexpr int kNSlotKvarNarrow = 7;
+constexpr int kNSlotUniformNarrow = 8;
 constexpr int kMaxChunks = 256;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
@@ -128,11 +132,10 @@ __device__ __forceinline__ float2 lds2_at_use(const float* p) {
   return make_float2(q->x, q->y);
 }
 
-// FP32x2 arithmetic (sm_100 packed add/mul/fma): a thread owns 4 adjacent columns and applies
-// the same operation to all of them, so columns (0,1) and (2,3) go through one instruction each.
-// Each component is rounded to nearest with denormals flushed, exactly like the scalar
-// operations under -use_fast_math, so every column gets the scalar result. a - b is issued as
-// fma(b, -1, a), which rounds once like a subtraction.
+// FP32x2 arithmetic (sm_100 packed add/mul/fma): a thread owns NC adjacent columns (4, or 2 in
+// the narrow-thread form) and applies the same operation to all of them, so each pair of columns
+// goes through one instruction. Each component is rounded to nearest with denormals flushed,
+// exactly like the scalar operations under -use_fast_math, so every column gets the scalar result.
 __device__ __forceinline__ uint64_t pk2(float a, float b) {
   uint64_t r;
   asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
@@ -159,40 +162,43 @@ __device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
   asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
   return r;
 }
-// d = a op b over the 4 columns; a float2 operand is the same pair for both halves
-#define FIP_V2(name, op)                                                                   \
-  __device__ __forceinline__ void name(float (&d)[4], const float (&a)[4], const float (&b)[4]) { \
-    un2(op(pk2(a[0], a[1]), pk2(b[0], b[1])), d[0], d[1]);                                \
-    un2(op(pk2(a[2], a[3]), pk2(b[2], b[3])), d[2], d[3]);                                \
-  }                                                                                        \
-  __device__ __forceinline__ void name(float (&d)[4], const float (&a)[4], float2 b) {    \
-    const uint64_t bb = pk2(b.x, b.y);                                                     \
-    un2(op(pk2(a[0], a[1]), bb), d[0], d[1]);                                              \
-    un2(op(pk2(a[2], a[3]), bb), d[2], d[3]);                                              \
-  }                                                                                        \
-  __device__ __forceinline__ void name(float (&d)[4], float2 a, const float (&b)[4]) {    \
-    const uint64_t aa = pk2(a.x, a.y);                                                     \
-    un2(op(aa, pk2(b[0], b[1])), d[0], d[1]);                                              \
-    un2(op(aa, pk2(b[2], b[3])), d[2], d[3]);                                              \
+// d = a op b over the N columns; a float2 operand is the same pair for every pair of columns
+#define FIP_V2(name, op)                                                                                  \
+  template <int N>                                                                                        \
+  __device__ __forceinline__ void name(float (&d)[N], const float (&a)[N], const float (&b)[N]) {         \
+    _Pragma("unroll") for (int i = 0; i < N; i += 2) un2(op(pk2(a[i], a[i + 1]), pk2(b[i], b[i + 1])), d[i], d[i + 1]); \
+  }                                                                                                       \
+  template <int N>                                                                                        \
+  __device__ __forceinline__ void name(float (&d)[N], const float (&a)[N], float2 b) {                    \
+    const uint64_t bb = pk2(b.x, b.y);                                                                    \
+    _Pragma("unroll") for (int i = 0; i < N; i += 2) un2(op(pk2(a[i], a[i + 1]), bb), d[i], d[i + 1]);   \
+  }                                                                                                       \
+  template <int N>                                                                                        \
+  __device__ __forceinline__ void name(float (&d)[N], float2 a, const float (&b)[N]) {                    \
+    const uint64_t aa = pk2(a.x, a.y);                                                                    \
+    _Pragma("unroll") for (int i = 0; i < N; i += 2) un2(op(aa, pk2(b[i], b[i + 1])), d[i], d[i + 1]);   \
   }
 FIP_V2(vadd, add2)
 FIP_V2(vsub, sub2)
 FIP_V2(vmul, mul2)
 #undef FIP_V2
 // d = a * b + c
-__device__ __forceinline__ void vfma(float (&d)[4], const float (&a)[4], const float (&b)[4], const float (&c)[4]) {
-  un2(fma2(pk2(a[0], a[1]), pk2(b[0], b[1]), pk2(c[0], c[1])), d[0], d[1]);
-  un2(fma2(pk2(a[2], a[3]), pk2(b[2], b[3]), pk2(c[2], c[3])), d[2], d[3]);
+template <int N>
+__device__ __forceinline__ void vfma(float (&d)[N], const float (&a)[N], const float (&b)[N], const float (&c)[N]) {
+#pragma unroll
+  for (int i = 0; i < N; i += 2) un2(fma2(pk2(a[i], a[i + 1]), pk2(b[i], b[i + 1]), pk2(c[i], c[i + 1])), d[i], d[i + 1]);
 }
-__device__ __forceinline__ void vfma(float (&d)[4], const float (&a)[4], float2 b, const float (&c)[4]) {
+template <int N>
+__device__ __forceinline__ void vfma(float (&d)[N], const float (&a)[N], float2 b, const float (&c)[N]) {
   const uint64_t bb = pk2(b.x, b.y);
-  un2(fma2(pk2(a[0], a[1]), bb, pk2(c[0], c[1])), d[0], d[1]);
-  un2(fma2(pk2(a[2], a[3]), bb, pk2(c[2], c[3])), d[2], d[3]);
+#pragma unroll
+  for (int i = 0; i < N; i += 2) un2(fma2(pk2(a[i], a[i + 1]), bb, pk2(c[i], c[i + 1])), d[i], d[i + 1]);
 }
-__device__ __forceinline__ void vfma(float (&d)[4], float2 a, const float (&b)[4], const float (&c)[4]) {
+template <int N>
+__device__ __forceinline__ void vfma(float (&d)[N], float2 a, const float (&b)[N], const float (&c)[N]) {
   const uint64_t aa = pk2(a.x, a.y);
-  un2(fma2(aa, pk2(b[0], b[1]), pk2(c[0], c[1])), d[0], d[1]);
-  un2(fma2(aa, pk2(b[2], b[3]), pk2(c[2], c[3])), d[2], d[3]);
+#pragma unroll
+  for (int i = 0; i < N; i += 2) un2(fma2(aa, pk2(b[i], b[i + 1]), pk2(c[i], c[i + 1])), d[i], d[i + 1]);
 }
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
@@ -230,9 +236,46 @@ __device__ __forceinline__ float pow_inv(float a) {
 #endif
 }
 
-template <int FB = kFieldBytes>
-__device__ __forceinline__ float4 lds4(const unsigned char* slot, int field, int col) {
-  return *reinterpret_cast<const float4*>(slot + field * FB + col * 4);
+// The NC staged values of `field` at staged column `col` of a ring slot (one 16- or 8-byte
+// shared-memory load)
+template <int NC, int FB>
+__device__ __forceinline__ void ldsv(float (&v)[NC], const unsigned char* slot, int field, int col) {
+  if constexpr (NC == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(slot + field * FB + col * 4);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  } else {
+    const float2 t = *reinterpret_cast<const float2*>(slot + field * FB + col * 4);
+    v[0] = t.x;
+    v[1] = t.y;
+  }
+}
+// NC values to global memory in one 16- or 8-byte store (p aligned to NC floats)
+template <int NC>
+__device__ __forceinline__ void stgv(float* p, const float (&v)[NC]) {
+  if constexpr (NC == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  else *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+}
+// hmax = max(hmax, h) over NC cells (p aligned to NC floats)
+template <int NC>
+__device__ __forceinline__ void hmax_foldv(float* p, const float (&h)[NC]) {
+  if constexpr (NC == 4) {
+    float4* q = reinterpret_cast<float4*>(p);
+    float4 m = *q;
+    m.x = fmaxf(m.x, h[0]);
+    m.y = fmaxf(m.y, h[1]);
+    m.z = fmaxf(m.z, h[2]);
+    m.w = fmaxf(m.w, h[3]);
+    *q = m;
+  } else {
+    float2* q = reinterpret_cast<float2*>(p);
+    float2 m = *q;
+    m.x = fmaxf(m.x, h[0]);
+    m.y = fmaxf(m.y, h[1]);
+    *q = m;
+  }
 }
 
 // Walk of a CTA's share of the active-tile row stream: maximal runs of rows that are
@@ -317,25 +360,44 @@ __device__ __forceinline__ bool next_run_ens(Walk& w, const int* list, const int
   return false;
 }
 
-// KW consumer warps per CTA (tiles of 120 * KW columns, TRT rows); ENS: the grid is a packed
-// ensemble (member table in the arguments, per-member dt, rows, sizes and CFL slots). The tile
-// height is a template argument so that the row-to-tile arithmetic compiles to shifts and masks.
-template <bool KVAR, bool ENS, int KW, int TRT>
-__global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
+// KW consumer warps per CTA, NC columns per thread (tiles of 30 * NC * KW columns, TRT rows); ENS:
+// the grid is a packed ensemble (member table in the arguments, per-member dt, rows, sizes and CFL
+// slots). The tile height is a template argument so that the row-to-tile arithmetic compiles to
+// shifts and masks. NC = 2 halves the registers a thread holds, so more CTAs fit on an SM.
+template <int NC, int KW>
+struct StepShape {
+  static_assert(NC == 2 || NC == 4, "4 or 2 columns per thread");
+  static_assert(KW == 2 || KW == 4, "tiles of 2 or 4 consumer warps");
+  static constexpr int kCols = 32 * NC * KW;       // staged columns per row and field
+  static constexpr int kFB = kCols * 4;            // bytes of one staged row of one field
+  static constexpr int kBoxes = kCols / 256;       // TMA boxes of 256 floats per staged row
+  static constexpr int TC = 30 * NC * KW;          // tile columns (lanes 1..30 of each warp store)
+  // staged column of the tile's column 0: lanes read [X0 - NC, X0 + TC + NC) of the staged row
+  // (the TMA x coordinate, column 0 - X0, stays a multiple of 4 floats)
+  static constexpr int X0 = (NC == 4 && KW == 4) ? FIP_SMEM_X0 : 4;
+  static constexpr int kMinCtas = NC == 4 ? (KW == 4 ? kMinCtas4 : kMinCtas2) : kMinCtasNarrow;
+  // ring depth in rows with and without the kSt field
+  static constexpr int kNSlotK = NC == 4 ? (KW == 4 ? kNSlotKvar : kNSlotKvar2) : kNSlotKvarNarrow;
+  static constexpr int kNSlotU = NC == 4 ? (KW == 4 ? kNSlotUniform : kNSlotUniform2) : kNSlotUniformNarrow;
+  static_assert(kBoxes >= 1 && kCols % 256 == 0, "staged rows are whole 256-float TMA boxes");
+  static_assert(X0 >= NC && X0 + TC + NC <= kCols && X0 % 4 == 0, "staged window");
+};
+
+template <bool KVAR, bool ENS, int KW, int TRT, int NC>
+__global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
     rmg_step_kernel(const __grid_constant__ CUtensorMap tm_h0, const __grid_constant__ CUtensorMap tm_h1,
                     const __grid_constant__ CUtensorMap tm_qx0, const __grid_constant__ CUtensorMap tm_qx1,
                     const __grid_constant__ CUtensorMap tm_qy0, const __grid_constant__ CUtensorMap tm_qy1,
                     const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_k,
                     const StepArgs a) {
+  using S = StepShape<NC, KW>;
   constexpr int NF = KVAR ? 5 : 4;
-  constexpr int kNSlot = KW == 4 ? (KVAR ? kNSlotKvar : kNSlotUniform) : (KVAR ? kNSlotKvar2 : kNSlotUniform2);
-  constexpr int kFB = KW * 128 * 4;  // bytes of one staged row of one field
+  constexpr int kNSlot = KVAR ? S::kNSlotK : S::kNSlotU;
+  constexpr int kFB = S::kFB;
   constexpr int kSlotBytes = NF * kFB;
-  constexpr int TC = 120 * KW;       // tile columns
-  // staged column of the tile's column 0: lanes read [X0 - 4, X0 + 120 * KW + 4) of the staged
-  // 128 * KW columns (TMA x stays a multiple of 4 floats either way)
-  constexpr int X0 = KW == 2 ? 4 : FIP_SMEM_X0;
-  static_assert(KW == 2 || KW == 4, "tiles of 2 or 4 consumer warps");
+  constexpr int TC = S::TC;
+  constexpr int X0 = S::X0;
+  constexpr int FULL = (1 << NC) - 1;  // all NC cells of a thread
   static_assert(kNSlot <= kNSlotMax, "ring depth");
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   __shared__ __align__(8) uint64_t full_bar[kNSlotMax];
@@ -373,9 +435,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       s_tbase[i] = i < a.n_members ? a.members[i].tile_base : a.n_tiles;
   }
   if (tid < 32) {  // prefix over the chunk counts of this step's plan
-    const int par = ctl->parity;
     const int* cnt = a.chunk_cnt[(ctl->iteration) & 1];
-    (void)par;
     if (lane == 0) {
       int acc = 0;
       for (int c = 0; c < a.n_chunks; ++c) {
@@ -436,7 +496,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
           mbar_arrive_expect_tx(&full_bar[slot], kSlotBytes);
           const int y = y0 + j;
 #pragma unroll
-          for (int b = 0; b < KW / 2; ++b) {
+          for (int b = 0; b < S::kBoxes; ++b) {
             tma_row(dst + F_H * kFB + 1024 * b, th, x0 + 256 * b, y, &full_bar[slot]);
             tma_row(dst + F_QX * kFB + 1024 * b, tqx, x0 + 256 * b, y, &full_bar[slot]);
             tma_row(dst + F_QY * kFB + 1024 * b, tqy, x0 + 256 * b, y, &full_bar[slot]);
@@ -481,7 +541,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
     c_ndtdx = make_float2(-dtdx, -dtdx);
   };
   set_scalars();
-  const int scol = X0 - 4 + 120 * warp + 4 * lane;  // staged column of k = 0
+  const int scol = X0 - NC + 30 * NC * warp + NC * lane;  // staged column of k = 0
   const bool out_lane = (lane >= 1 && lane <= 30);
   float* const h_out = a.h[par ^ 1];
   float* const qx_out = a.qx[par ^ 1];
@@ -532,12 +592,12 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       }
       __syncwarp();
     }
-    const int c = s * TC - 4 + 120 * warp + 4 * lane;  // global column of k = 0
-    // 4-bit column masks of the cell sets the reference's kernel writes (src/kernels.cu:383-406)
+    const int c = s * TC - NC + 30 * NC * warp + NC * lane;  // global column of k = 0
+    // NC-bit column masks of the cell sets the reference's kernel writes (src/kernels.cu:383-406)
     int colHm = 0, colQXm = 0, colQYm = 0, colInm = 0;
-    bool holdX[4];
+    bool holdX[NC];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < NC; ++k) {
       const int cc = c + k;
       colHm |= (out_lane && cc >= 1 && cc <= W - 2) << k;
       colQXm |= (out_lane && cc >= 1 && cc <= W - 3) << k;
@@ -568,39 +628,34 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
     // ---- prologue: rows ra-2 .. ra ----
     // carried from row to row: only computed quantities; the raw fields of rows r-1 .. r+2 are
     // read from the staged rows again at every row
-    float ux0[4], uxW0, uy0[4], uyE0, uyS[4], gxS[4], gy0[4], qy2S[4];
-    float lim0[4], limE0;  // h * dt_inv * dx * 0.25f of row r (and its east neighbour)
+    float ux0[NC], uxW0, uy0[NC], uyE0, uyS[NC], gxS[NC], gy0[NC], qy2S[NC];
+    float lim0[NC], limE0;  // h * dt_inv * dx * 0.25f of row r (and its east neighbour)
     {
       const unsigned char* slA = ring + iS * kSlotBytes;
       const unsigned char* slB = ring + i0 * kSlotBytes;
       const unsigned char* slC = ring + i1 * kSlotBytes;
-      const float4 vhs = lds4<kFB>(slA, F_H, scol);
-      const float4 vqys = lds4<kFB>(slA, F_QY, scol);
-      const float4 vh0 = lds4<kFB>(slB, F_H, scol);
-      const float4 vqx0 = lds4<kFB>(slB, F_QX, scol);
-      const float4 vqy0 = lds4<kFB>(slB, F_QY, scol);
-      const float4 vh1 = lds4<kFB>(slC, F_H, scol);
-      const float hs[4] = {vhs.x, vhs.y, vhs.z, vhs.w};
-      const float qyS[4] = {vqys.x, vqys.y, vqys.z, vqys.w};
-      const float h0[4] = {vh0.x, vh0.y, vh0.z, vh0.w};
-      const float qx0[4] = {vqx0.x, vqx0.y, vqx0.z, vqx0.w};
-      const float qy0[4] = {vqy0.x, vqy0.y, vqy0.z, vqy0.w};
-      const float h1[4] = {vh1.x, vh1.y, vh1.z, vh1.w};
+      float hs[NC], qyS[NC], h0[NC], qx0[NC], qy0[NC], h1[NC];
+      ldsv<NC, kFB>(hs, slA, F_H, scol);
+      ldsv<NC, kFB>(qyS, slA, F_QY, scol);
+      ldsv<NC, kFB>(h0, slB, F_H, scol);
+      ldsv<NC, kFB>(qx0, slB, F_QX, scol);
+      ldsv<NC, kFB>(qy0, slB, F_QY, scol);
+      ldsv<NC, kFB>(h1, slC, F_H, scol);
       const float hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < NC; ++k) {
         uyS[k] = qyS[k] / fmax3(kDH, hs[k], h0[k]);
-        ux0[k] = qx0[k] / fmax3(kDH, h0[k], k < 3 ? h0[k + 1] : hE0);
+        ux0[k] = qx0[k] / fmax3(kDH, h0[k], k < NC - 1 ? h0[k + 1] : hE0);
         uy0[k] = qy0[k] / fmax3(kDH, h0[k], h1[k]);
       }
       vmul(lim0, h0, c_dti);
       vmul(lim0, lim0, c_dx);
       vmul(lim0, lim0, c_q);
-      uxW0 = __shfl_up_sync(0xffffffffu, ux0[3], 1);
+      uxW0 = __shfl_up_sync(0xffffffffu, ux0[NC - 1], 1);
       uyE0 = __shfl_down_sync(0xffffffffu, uy0[0], 1);
       limE0 = __shfl_down_sync(0xffffffffu, lim0[0], 1);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < NC; ++k) {
         // compute_rmg_gy for row ra-1: uy_i = uy(ra-1), uy_south = uy(ra-2)
         gy0[k] = (uy0[k] + uyS[k] > 0) ? qyS[k] * uyS[k] : qy0[k] * uy0[k];
         gxS[k] = 0.f;
@@ -623,191 +678,180 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       const unsigned char* sl0 = ring + i0 * kSlotBytes;
       const unsigned char* sl1 = ring + i1 * kSlotBytes;
       const unsigned char* sl2 = ring + i2 * kSlotBytes;
-      float h2r[4], qx1[4], qy1[4], s1[4], fric[4], qyS[4], s0[4], h0[4], h1[4], qx0[4], qy0[4];
-      {
-        const float4 vqs = lds4<kFB>(slS, F_QY, scol);
-        const float4 vs0 = lds4<kFB>(sl0, F_S, scol);
-        const float4 vh0 = lds4<kFB>(sl0, F_H, scol);
-        const float4 vqx0 = lds4<kFB>(sl0, F_QX, scol);
-        const float4 vqy0 = lds4<kFB>(sl0, F_QY, scol);
-        const float4 vh1 = lds4<kFB>(sl1, F_H, scol);
-        qyS[0] = vqs.x; qyS[1] = vqs.y; qyS[2] = vqs.z; qyS[3] = vqs.w;
-        s0[0] = vs0.x; s0[1] = vs0.y; s0[2] = vs0.z; s0[3] = vs0.w;
-        h0[0] = vh0.x; h0[1] = vh0.y; h0[2] = vh0.z; h0[3] = vh0.w;
-        qx0[0] = vqx0.x; qx0[1] = vqx0.y; qx0[2] = vqx0.z; qx0[3] = vqx0.w;
-        qy0[0] = vqy0.x; qy0[1] = vqy0.y; qy0[2] = vqy0.z; qy0[3] = vqy0.w;
-        h1[0] = vh1.x; h1[1] = vh1.y; h1[2] = vh1.z; h1[3] = vh1.w;
-        const float4 v2 = lds4<kFB>(sl2, F_H, scol);
-        const float4 vqx = lds4<kFB>(sl1, F_QX, scol);
-        const float4 vqy = lds4<kFB>(sl1, F_QY, scol);
-        const float4 vs = lds4<kFB>(sl1, F_S, scol);
-        h2r[0] = v2.x; h2r[1] = v2.y; h2r[2] = v2.z; h2r[3] = v2.w;
-        qx1[0] = vqx.x; qx1[1] = vqx.y; qx1[2] = vqx.z; qx1[3] = vqx.w;
-        qy1[0] = vqy.x; qy1[1] = vqy.y; qy1[2] = vqy.z; qy1[3] = vqy.w;
-        s1[0] = vs.x; s1[1] = vs.y; s1[2] = vs.z; s1[3] = vs.w;
-        if (KVAR) {
-          const float4 vk = lds4<kFB>(sl0, F_K, scol);
-          float kk[4] = {vk.x, vk.y, vk.z, vk.w};
+      float h2r[NC], qx1[NC], qy1[NC], s1[NC], fric[NC], qyS[NC], s0[NC], h0[NC], h1[NC], qx0[NC], qy0[NC];
+      ldsv<NC, kFB>(qyS, slS, F_QY, scol);
+      ldsv<NC, kFB>(s0, sl0, F_S, scol);
+      ldsv<NC, kFB>(h0, sl0, F_H, scol);
+      ldsv<NC, kFB>(qx0, sl0, F_QX, scol);
+      ldsv<NC, kFB>(qy0, sl0, F_QY, scol);
+      ldsv<NC, kFB>(h1, sl1, F_H, scol);
+      ldsv<NC, kFB>(h2r, sl2, F_H, scol);
+      ldsv<NC, kFB>(qx1, sl1, F_QX, scol);
+      ldsv<NC, kFB>(qy1, sl1, F_QY, scol);
+      ldsv<NC, kFB>(s1, sl1, F_S, scol);
+      if (KVAR) {
+        float kk[NC];
+        ldsv<NC, kFB>(kk, sl0, F_K, scol);
 #if FIP_VAR_IK2
-          const float g = ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg;  // the field holds 1 / kSt^2
-          vmul(fric, kk, make_float2(g, g));
+        const float g = ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg;  // the field holds 1 / kSt^2
+        vmul(fric, kk, make_float2(g, g));
 #else
-          vmul(kk, kk, kk);
+        vmul(kk, kk, kk);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) fric[k] = (ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg) / kk[k];
+        for (int k = 0; k < NC; ++k) fric[k] = (ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg) / kk[k];
 #endif
-        } else {
-          fric[0] = fric[1] = fric[2] = fric[3] = ENS ? ldsf_at_use(&s_mcf[warp][10]) : fric_u;
-        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < NC; ++k) fric[k] = ENS ? ldsf_at_use(&s_mcf[warp][10]) : fric_u;
       }
       const float hE0 = __shfl_down_sync(0xffffffffu, h0[0], 1);
       const float hE1 = __shfl_down_sync(0xffffffffu, h1[0], 1);
-      const float qxW0 = __shfl_up_sync(0xffffffffu, qx0[3], 1);
+      const float qxW0 = __shfl_up_sync(0xffffffffu, qx0[NC - 1], 1);
       const float qyE0 = __shfl_down_sync(0xffffffffu, qy0[0], 1);
       const float qySE = __shfl_down_sync(0xffffffffu, qyS[0], 1);
       const float sE0 = __shfl_down_sync(0xffffffffu, s0[0], 1);
-      const float qxW1 = __shfl_up_sync(0xffffffffu, qx1[3], 1);
-      float t[4], u[4];
+      const float qxW1 = __shfl_up_sync(0xffffffffu, qx1[NC - 1], 1);
+      float t[NC], u[NC];
 
       // velocities of row r+1 (src/kernels.cu:351-354) and the clamp factors of row r+1
-      float ux1[4], uy1[4], lim1[4];
+      float ux1[NC], uy1[NC], lim1[NC];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        ux1[k] = qx1[k] / fmax3(kDH, h1[k], k < 3 ? h1[k + 1] : hE1);
+      for (int k = 0; k < NC; ++k) {
+        ux1[k] = qx1[k] / fmax3(kDH, h1[k], k < NC - 1 ? h1[k + 1] : hE1);
         uy1[k] = qy1[k] / fmax3(kDH, h1[k], h2r[k]);
       }
       vmul(lim1, h1, ENS ? lds2_at_use(&s_mcf[warp][0]) : c_dti);
       vmul(lim1, lim1, ENS ? lds2_at_use(&s_mcf[warp][2]) : c_dx);
       vmul(lim1, lim1, c_q);
-      const float ux1W = __shfl_up_sync(0xffffffffu, ux1[3], 1);
+      const float ux1W = __shfl_up_sync(0xffffffffu, ux1[NC - 1], 1);
       const float uy1E = __shfl_down_sync(0xffffffffu, uy1[0], 1);
 
-      float fx[4], fy[4], gx[4], gy1[4];
+      float fx[NC], fy[NC], gx[NC], gy1[NC];
       // compute_rmg_fy (:45-54): ux at the cell and its north neighbour
       vadd(t, ux0, ux1);
       vmul(u, t, c_h);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) fy[k] = t[k] > 0 ? qy0[k] : (k < 3 ? qy0[k + 1] : qyE0);
+      for (int k = 0; k < NC; ++k) fy[k] = t[k] > 0 ? qy0[k] : (k < NC - 1 ? qy0[k + 1] : qyE0);
       vmul(fy, fy, u);
       // compute_rmg_gy for row r+1 (:65-73, called at :359)
       vadd(t, uy1, uy0);
       vmul(u, qy0, uy0);
       vmul(gy1, qy1, uy1);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) gy1[k] = t[k] > 0 ? u[k] : gy1[k];
+      for (int k = 0; k < NC; ++k) gy1[k] = t[k] > 0 ? u[k] : gy1[k];
       // compute_rmg_gx (:35-43)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) t[k] = uy0[k] + (k < 3 ? uy0[k + 1] : uyE0);
+      for (int k = 0; k < NC; ++k) t[k] = uy0[k] + (k < NC - 1 ? uy0[k + 1] : uyE0);
       vmul(u, t, c_h);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) gx[k] = t[k] > 0 ? qx0[k] : qx1[k];
+      for (int k = 0; k < NC; ++k) gx[k] = t[k] > 0 ? qx0[k] : qx1[k];
       vmul(gx, gx, u);
       // compute_rmg_fx (:56-63): qx * ux of the cell or of its west neighbour
       vmul(u, qx0, ux0);
       const float pqW = qxW0 * uxW0;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < NC; ++k) {
         const float uw = k > 0 ? ux0[k - 1] : uxW0;
         fx[k] = (uw + ux0[k] > 0) ? (k > 0 ? u[k - 1] : pqW) : u[k];
       }
-      const float fyW = __shfl_up_sync(0xffffffffu, fy[3], 1);
+      const float fyW = __shfl_up_sync(0xffffffffu, fy[NC - 1], 1);
       const float fxE = __shfl_down_sync(0xffffffffu, fx[0], 1);
 
       const int Hr = ENS ? lds_at_use(&s_msc[warp][0]) : H;
       const bool hold_y = (r == 0 || r == Hr - 2);
       // face depths and the mean cross discharges of the friction factor (:83-92, :110-119)
-      float ax0[4], ax1[4], ay0[4], ay1[4], uyx[4], uxy[4];
+      float ax0[NC], ax1[NC], ay0[NC], ay1[NC], uyx[NC], uxy[NC];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) t[k] = h0[k] + (k < 3 ? h0[k + 1] : hE0);
+      for (int k = 0; k < NC; ++k) t[k] = h0[k] + (k < NC - 1 ? h0[k + 1] : hE0);
       vmul(ax0, t, c_h);
       vadd(t, h0, h1);
       vmul(ay0, t, c_h);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < NC; ++k) {
         ax0[k] = fmaxf(0.f, ax0[k]);
         ax1[k] = fmaxf(ax0[k], kDH);
         ay0[k] = fmaxf(0.f, ay0[k]);
         ay1[k] = fmaxf(ay0[k], kDH);
       }
 #pragma unroll
-      for (int k = 0; k < 4; ++k) t[k] = qy0[k] + (k < 3 ? qy0[k + 1] : qyE0);
+      for (int k = 0; k < NC; ++k) t[k] = qy0[k] + (k < NC - 1 ? qy0[k + 1] : qyE0);
       vadd(t, t, qyS);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) t[k] = t[k] + (k < 3 ? qyS[k + 1] : qySE);
+      for (int k = 0; k < NC; ++k) t[k] = t[k] + (k < NC - 1 ? qyS[k + 1] : qySE);
       vmul(uyx, t, c_q);
       vadd(t, qx0, qx1);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) t[k] = (t[k] + (k > 0 ? qx0[k - 1] : qxW0)) + (k > 0 ? qx1[k - 1] : qxW1);
+      for (int k = 0; k < NC; ++k) t[k] = (t[k] + (k > 0 ? qx0[k - 1] : qxW0)) + (k > 0 ? qx1[k - 1] : qxW1);
       vmul(uxy, t, c_q);
       // friction factors fric * sqrt(ux^2 + uy^2) * (1 / a1)^2.33 (:91-94, :118-121), 0 where both
       // discharges vanish (then the square sum is 0 and the product is 0 for every finite fric)
-      float rx[4], ry[4];
+      float rx[NC], ry[NC];
       {
-        float mx[4], my[4];
+        float mx[NC], my[NC];
         vmul(t, uyx, uyx);
         vfma(mx, qx0, qx0, t);
         vmul(t, qy0, qy0);
         vfma(my, uxy, uxy, t);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < NC; ++k) {
           t[k] = sqrtf(mx[k]);
           u[k] = pow_inv(ax1[k]);
         }
         vmul(rx, fric, t);
         vmul(rx, rx, u);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < NC; ++k) {
           t[k] = sqrtf(my[k]);
           u[k] = pow_inv(ay1[k]);
         }
         vmul(ry, fric, t);
         vmul(ry, ry, u);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < NC; ++k) {
           rx[k] = (mx[k] == 0.f) ? 0.f : rx[k];
           ry[k] = (my[k] == 0.f) ? 0.f : ry[k];
         }
       }
       // compute_rmg_qx / compute_rmg_qy (:75-127): the same expression trees; 0.5 G h^2 as
       // nhh = (-0.5 G h) h = -(0.5 G h h)
-      float qx2[4], qy2[4];
+      float qx2[NC], qy2[NC];
       {
-        float nch[4], nhh[4], dsum[4];
+        float nch[NC], nhh[NC], dsum[NC];
         vmul(nch, h0, c_nhg);
         vmul(nhh, nch, h0);
         const float nchE = -kHG * hE0;
         // x: -dfx - dgx - dhx + dhg
 #pragma unroll
-        for (int k = 0; k < 4; ++k) t[k] = (k < 3 ? fx[k + 1] : fxE) - fx[k];
+        for (int k = 0; k < NC; ++k) t[k] = (k < NC - 1 ? fx[k + 1] : fxE) - fx[k];
         vmul(dsum, t, c_ndxi);                  // -dfx
         vsub(t, gx, gxS);                       // (gx_i - gx_south)
         vfma(dsum, t, c_ndxi, dsum);            // - dgx
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          t[k] = fmaf(-(k < 3 ? nch[k + 1] : nchE), k < 3 ? h0[k + 1] : hE0, nhh[k]);  // 0.5G hE hE - 0.5G h h
+        for (int k = 0; k < NC; ++k) {
+          t[k] = fmaf(-(k < NC - 1 ? nch[k + 1] : nchE), k < NC - 1 ? h0[k + 1] : hE0, nhh[k]);  // 0.5G hE hE - 0.5G h h
         }
         vfma(dsum, t, c_ndxi, dsum);            // - dhx
 #pragma unroll
-        for (int k = 0; k < 4; ++k) u[k] = s0[k] - (k < 3 ? s0[k + 1] : sE0);  // -s_east + s_i
+        for (int k = 0; k < NC; ++k) u[k] = s0[k] - (k < NC - 1 ? s0[k + 1] : sE0);  // -s_east + s_i
         vmul(t, ax0, c_g);
         vmul(t, t, u);
         vfma(dsum, t, ENS ? lds2_at_use(&s_mcf[warp][4]) : c_dxi, dsum);  // + dhg
         vfma(dsum, ENS ? lds2_at_use(&s_mcf[warp][6]) : c_dt, dsum, qx0);  // qx + dt * (...)
         vadd(t, c_one, rx);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) qx2[k] = dsum[k] / t[k];
+        for (int k = 0; k < NC; ++k) qx2[k] = dsum[k] / t[k];
         vadd(qx2, qx2, c_zero);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < NC; ++k) {
           float q = fminf(qx2[k], lim0[k]);
-          q = fmaxf(q, -(k < 3 ? lim0[k + 1] : limE0));
+          q = fmaxf(q, -(k < NC - 1 ? lim0[k + 1] : limE0));
           qx2[k] = holdX[k] ? qx0[k] : q;  // boundary-face holds (:373-376)
         }
         // y: -dgy - dfy - dhy + dhg
         vsub(t, gy1, gy0);
         vmul(dsum, t, c_ndxi);                  // -dgy
 #pragma unroll
-        for (int k = 0; k < 4; ++k) t[k] = fy[k] - (k > 0 ? fy[k - 1] : fyW);
+        for (int k = 0; k < NC; ++k) t[k] = fy[k] - (k > 0 ? fy[k - 1] : fyW);
         vfma(dsum, t, c_ndxi, dsum);            // - dfy
         vmul(u, h1, c_hg);
         vfma(t, u, h1, nhh);                    // 0.5G hN hN - 0.5G h h
@@ -819,16 +863,16 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
         vfma(dsum, ENS ? lds2_at_use(&s_mcf[warp][6]) : c_dt, dsum, qy0);  // qy + dt * (...)
         vadd(t, c_one, ry);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) qy2[k] = dsum[k] / t[k];
+        for (int k = 0; k < NC; ++k) qy2[k] = dsum[k] / t[k];
         vadd(qy2, qy2, c_zero);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < NC; ++k) {
           float q = fminf(qy2[k], lim0[k]);
           q = fmaxf(q, -lim1[k]);
           qy2[k] = hold_y ? qy0[k] : q;
         }
       }
-      const float qx2W = __shfl_up_sync(0xffffffffu, qx2[3], 1);
+      const float qx2W = __shfl_up_sync(0xffffffffu, qx2[NC - 1], 1);
 
       {
         const bool store_row = r >= ra;  // the extra row below a run only feeds qy2S
@@ -836,74 +880,68 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
         const float nvr = ENS ? __int_as_float(lds_at_use(&s_msc[warp][4])) : nv;
         const int Hs = ENS ? lds_at_use(&s_msc[warp][0]) : H;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) validm |= (s0[k] != nvr) << k;
+        for (int k = 0; k < NC; ++k) validm |= (s0[k] != nvr) << k;
         const int mH = (store_row && r >= 1 && r <= Hs - 2) ? (colHm & validm) : 0;
         const int mQX = (store_row && r >= 2 && r <= Hs - 3) ? (colQXm & validm) : 0;
         const int mQY = (store_row && r >= 1 && r <= Hs - 3) ? (colQYm & validm) : 0;
         // continuity (:381): h - dt * dx_inv * ((qx_i - qx_W) + (qy_i - qy_S))
-        float h2[4];
+        float h2[NC];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) t[k] = qx2[k] - (k > 0 ? qx2[k - 1] : qx2W);
+        for (int k = 0; k < NC; ++k) t[k] = qx2[k] - (k > 0 ? qx2[k - 1] : qx2W);
         vsub(u, qy2, qy2S);
         vadd(t, t, u);
         vfma(h2, ENS ? lds2_at_use(&s_mcf[warp][8]) : c_ndtdx, t, h0);
         // CFL of wet stored cells (:392-396): dx / (sqrt(G h') + max |u|), velocities of the old state
         vmul(t, c_g, h2);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < NC; ++k) {
           const float uw = k > 0 ? ux0[k - 1] : uxW0;
           u[k] = fmaxf(fabsf(uy0[k]), fmaxf(fabsf(uyS[k]), fmaxf(fabsf(ux0[k]), fabsf(uw))));
           t[k] = sqrtf(t[k]);
         }
         vadd(t, t, u);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < NC; ++k) {
           const bool wk = (mH >> k) & 1;
           expacc = max(expacc, __float_as_uint(h2[k]) & 0x7f800000u);  // all-ones exponent: NaN/Inf
           den_max = fmaxf(den_max, (wk && h2[k] > kEPS) ? t[k] : 0.0f);
           nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & 0x7fffffffu;
         }
         const size_t row_off = (size_t)(r + (ENS ? lds_at_use(&s_msc[warp][1]) : 0)) * (size_t)pitch + (size_t)c;
-        if (mH == 15) {
-          *reinterpret_cast<float4*>(h_out + row_off) = make_float4(h2[0], h2[1], h2[2], h2[3]);
+        if (mH == FULL) {
+          stgv<NC>(h_out + row_off, h2);
         } else {
 #pragma unroll
-          for (int k = 0; k < 4; ++k)
+          for (int k = 0; k < NC; ++k)
             if ((mH >> k) & 1) h_out[row_off + k] = h2[k];
         }
-        if (mQX == 15) {
-          *reinterpret_cast<float4*>(qx_out + row_off) = make_float4(qx2[0], qx2[1], qx2[2], qx2[3]);
+        if (mQX == FULL) {
+          stgv<NC>(qx_out + row_off, qx2);
         } else {
 #pragma unroll
-          for (int k = 0; k < 4; ++k)
+          for (int k = 0; k < NC; ++k)
             if ((mQX >> k) & 1) qx_out[row_off + k] = qx2[k];
         }
-        if (mQY == 15) {
-          *reinterpret_cast<float4*>(qy_out + row_off) = make_float4(qy2[0], qy2[1], qy2[2], qy2[3]);
+        if (mQY == FULL) {
+          stgv<NC>(qy_out + row_off, qy2);
         } else {
 #pragma unroll
-          for (int k = 0; k < 4; ++k)
+          for (int k = 0; k < NC; ++k)
             if ((mQY >> k) & 1) qy_out[row_off + k] = qy2[k];
         }
         if (fold && store_row) {  // flood_plains_kernel on the post-boundary state of the last step (:254-262)
-          if (colInm == 15) {
-            float4* hm = reinterpret_cast<float4*>(a.hmax + row_off);
-            float4 m = *hm;
-            m.x = fmaxf(m.x, h0[0]);
-            m.y = fmaxf(m.y, h0[1]);
-            m.z = fmaxf(m.z, h0[2]);
-            m.w = fmaxf(m.w, h0[3]);
-            *hm = m;
+          if (colInm == FULL) {
+            hmax_foldv<NC>(a.hmax + row_off, h0);
           } else {
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
+            for (int k = 0; k < NC; ++k)
               if ((colInm >> k) & 1) a.hmax[row_off + k] = fmaxf(a.hmax[row_off + k], h0[k]);
           }
         }
         // per-tile wet flag for the next plan, flushed at the tile's last row
         if (store_row && ((r + 1) % TR == 0 || r + 1 == rb)) {
-          // halo lanes hold the neighbouring strips' cells; columns beyond W only occur in the last
-          // strip, whose tiles are always computed anyway
+          // halo lanes hold the neighbouring strips' cells; columns beyond W (zero-filled loads)
+          // can only set flags, never clear them
           if (__any_sync(0xffffffffu, out_lane && nzacc != 0u) && lane == 0) {
             const int tb = ENS ? lds_at_use(&s_msc[warp][2]) : 0, nt = ENS ? lds_at_use(&s_msc[warp][3]) : nty;
             nzs[tb + s * nt + r / TR] = 1;
@@ -925,7 +963,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, KW == 4 ? kMinCtas : kMinCtas2)
       }
       // travel north (:408-433)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < NC; ++k) {
         qy2S[k] = qy2[k];
         gxS[k] = gx[k];
         uyS[k] = uy0[k];
@@ -1116,8 +1154,8 @@ __global__ void sample_gather_kernel(const float* h, const float* qx, const floa
 
 }  // namespace
 
-void tile_geometry(int W, int H, int* n_sx, int* n_ty, int* n_tiles, int* n_chunks) {
-  *n_sx = (W + FIP_TILE_COLS - 1) / FIP_TILE_COLS;
+void tile_geometry(int W, int H, int tile_cols, int* n_sx, int* n_ty, int* n_tiles, int* n_chunks) {
+  *n_sx = (W + tile_cols - 1) / tile_cols;
   *n_ty = (H + FIP_TILE_ROWS - 1) / FIP_TILE_ROWS;
   *n_tiles = *n_sx * *n_ty;
   *n_chunks = (*n_tiles + FIP_PLAN_CHUNK - 1) / FIP_PLAN_CHUNK;
@@ -1167,19 +1205,21 @@ cudaError_t prepare_kst_field(float* kst, int W, int H, int pitch, cudaStream_t 
 #endif
 }
 
-int rmg_step_grid(int device) {
+int rmg_step_grid(int device, int nc) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return kMinCtas * sms;
+  return (nc == 2 ? kMinCtasNarrow : kMinCtas4) * sms;
 }
 
-template <bool KVAR, bool ENS, int KW, int TRT>
+int single_tile_cols(int nc) { return nc == 2 ? StepShape<2, 4>::TC : StepShape<4, 4>::TC; }
+
+template <bool KVAR, bool ENS, int KW, int TRT, int NC>
 static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t stream) {
+  using S = StepShape<NC, KW>;
   constexpr int NF = KVAR ? 5 : 4;
-  constexpr int kNSlot = KW == 4 ? (KVAR ? kNSlotKvar : kNSlotUniform) : (KVAR ? kNSlotKvar2 : kNSlotUniform2);
-  const int smem = kNSlot * NF * KW * 128 * 4 + 1024;
+  const int smem = (KVAR ? S::kNSlotK : S::kNSlotU) * NF * S::kFB + 1024;
   static std::atomic<uint64_t> configured{0};
-  const cudaError_t e = ensure_dynamic_smem(rmg_step_kernel<KVAR, ENS, KW, TRT>, smem, configured);
+  const cudaError_t e = ensure_dynamic_smem(rmg_step_kernel<KVAR, ENS, KW, TRT, NC>, smem, configured);
   if (e != cudaSuccess) return e;
   StepArgs a;
   for (int b = 0; b < 2; ++b) {
@@ -1205,7 +1245,7 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
   a.members = st.members;
   a.mctl = st.mctl;
   a.n_members = st.n_members;
-  rmg_step_kernel<KVAR, ENS, KW, TRT><<<grid, (KW + 1) * 32, smem, stream>>>(
+  rmg_step_kernel<KVAR, ENS, KW, TRT, NC><<<grid, (KW + 1) * 32, smem, stream>>>(
       st.tm_h[0], st.tm_h[1], st.tm_qx[0], st.tm_qx[1], st.tm_qy[0], st.tm_qy[1], st.tm_sohle, st.tm_kst, a);
   return cudaGetLastError();
 }
@@ -1213,14 +1253,19 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
 cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t stream) {
   if (st.n_chunks > kMaxChunks) return cudaErrorInvalidValue;
   constexpr int T = FIP_TILE_ROWS;
-  if (!st.members)
-    return st.kst ? launch_step_t<true, false, 4, T>(st, grid, stream) : launch_step_t<false, false, 4, T>(st, grid, stream);
+  if (!st.members) {
+    if (st.nc == 2)
+      return st.kst ? launch_step_t<true, false, 4, T, 2>(st, grid, stream)
+                    : launch_step_t<false, false, 4, T, 2>(st, grid, stream);
+    return st.kst ? launch_step_t<true, false, 4, T, 4>(st, grid, stream)
+                  : launch_step_t<false, false, 4, T, 4>(st, grid, stream);
+  }
   if (st.n_members > FIP_ENS_MAX_MEMBERS) return cudaErrorInvalidValue;
   // ensemble tile shapes: 2 or 4 consumer warps, 16, 32 or 64 rows
 #define FIP_ENS_LAUNCH(KW_, TR_)                                                                   \
   if (st.kw == KW_ && st.tile_rows == TR_)                                                         \
-    return st.kst ? launch_step_t<true, true, KW_, TR_>(st, grid, stream)                          \
-                  : launch_step_t<false, true, KW_, TR_>(st, grid, stream);
+    return st.kst ? launch_step_t<true, true, KW_, TR_, 4>(st, grid, stream)                       \
+                  : launch_step_t<false, true, KW_, TR_, 4>(st, grid, stream);
   FIP_ENS_LAUNCH(4, 32)
   FIP_ENS_LAUNCH(4, 16)
   FIP_ENS_LAUNCH(4, 64)
@@ -1234,12 +1279,12 @@ cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t strea
 int rmg_step_grid_kw(int device, int kw) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return (kw == 2 ? kMinCtas2 : kMinCtas) * sms;
+  return (kw == 2 ? kMinCtas2 : kMinCtas4) * sms;
 }
 
 cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t stream) {
   init_tiles_kernel<<<st.n_tiles, 256, 0, stream>>>(st.h[parity], st.qx[parity], st.qy[parity], st.sohle, st.W, st.H,
-                                                    st.pitch, st.no_value, st.n_ty, st.n_tiles, FIP_TILE_COLS,
+                                                    st.pitch, st.no_value, st.n_ty, st.n_tiles, st.tile_cols,
                                                     FIP_TILE_ROWS, st.force, nullptr, st.sticky, st.nz[0], st.nz[1]);
   return cudaGetLastError();
 }
@@ -1389,7 +1434,7 @@ extern "C" int fip_rmg_step_noalloc(const float* h_in, const float* qx_in, const
   if (pitch < W || (pitch % 4) != 0)
     return bad(-7, "fip_rmg_step_noalloc: pitch must be >= W and a multiple of 4 elements (16 bytes)");
   int n_sx, n_ty, n_tiles, n_chunks;
-  tile_geometry(W, H, &n_sx, &n_ty, &n_tiles, &n_chunks);
+  tile_geometry(W, H, FIP_TILE_COLS, &n_sx, &n_ty, &n_tiles, &n_chunks);
   if (n_tiles > kNoAllocMaxTiles)
     return bad(-7, "fip_rmg_step_noalloc: a " + std::to_string(W) + " x " + std::to_string(H) + " grid has " +
                        std::to_string(n_tiles) + " tiles of 480 x 32 cells; the static scratch holds at most " +
@@ -1441,7 +1486,7 @@ extern "C" int fip_rmg_step_noalloc(const float* h_in, const float* qx_in, const
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   noalloc_setup_kernel<<<(n_tiles + 255) / 256, 256, 0, s>>>(scratch, dt, n_tiles, n_chunks);
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = launch_rmg_step(st, rmg_step_grid(device), s);
+  if (e == cudaSuccess) e = launch_rmg_step(st, rmg_step_grid(device, 4), s);
   if (e == cudaSuccess && cfl_out_or_null) {
     noalloc_finish_kernel<<<1, 1, 0, s>>>(scratch, cfl_out_or_null);
     e = cudaGetLastError();

@@ -43,11 +43,16 @@ struct StencilState {
   int n_members = 0;
   int tile_rows = FIP_TILE_ROWS;
   int kw = 4;  // consumer warps per CTA: tiles of 120 * kw columns
+  int nc = 4;  // single grids: columns per thread (4, or 2: narrow threads)
+  int tile_cols = FIP_TILE_COLS;  // single grids: 30 * nc * 4
   TileForce force;  // single grids: tiles the boundary conditions keep active
 };
 
-// Geometry of the tile grid for a W x H domain.
-void tile_geometry(int W, int H, int* n_sx, int* n_ty, int* n_tiles, int* n_chunks);
+// Geometry of the tile grid for a W x H domain in tiles of tile_cols x FIP_TILE_ROWS cells.
+void tile_geometry(int W, int H, int tile_cols, int* n_sx, int* n_ty, int* n_tiles, int* n_chunks);
+
+// Tile columns of a single grid whose threads own nc columns (480 for 4, 240 for 2).
+int single_tile_cols(int nc);
 
 // Encodes the TMA descriptors of every field (box 256 x 1 floats). Returns a CUresult.
 int make_tensor_maps(StencilState* st);
@@ -91,7 +96,8 @@ cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, cons
 // Converts an uploaded kSt grid into the form the step kernel reads.
 cudaError_t prepare_kst_field(float* kst, int W, int H, int pitch, cudaStream_t stream);
 
-// Number of CTAs the step kernel runs with (3 per SM).
-int rmg_step_grid(int device);
+// Number of CTAs the single-grid step kernel runs with (3 per SM with 4 columns per thread, 5
+// with 2).
+int rmg_step_grid(int device, int nc);
 
 }  // namespace fip

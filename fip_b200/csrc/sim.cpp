@@ -14,6 +14,7 @@
 #include <cstdint>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <ctime>
 #include <fstream>
@@ -65,6 +66,12 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace fip
 
 namespace {
+// Columns per stencil thread of single grids: 4, or 2 with FIP_STENCIL_NC=2 in the environment
+int stencil_nc() {
+  const char* v = std::getenv("FIP_STENCIL_NC");
+  return (v && v[0] == '2' && v[1] == 0) ? 2 : 4;
+}
+
 // NVTX range for the lifetime of a scope (visible under Nsight Systems / ncu --nvtx; a no-op when
 // no tool is attached)
 struct Range {
@@ -215,7 +222,9 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
   st.dx = cfg.dx;
   st.kst_fixed = cfg.kst_fixed;
   st.no_value = cfg.no_data;
-  fip::tile_geometry(st.W, st.H, &st.n_sx, &st.n_ty, &st.n_tiles, &st.n_chunks);
+  st.nc = stencil_nc();
+  st.tile_cols = fip::single_tile_cols(st.nc);
+  fip::tile_geometry(st.W, st.H, st.tile_cols, &st.n_sx, &st.n_ty, &st.n_tiles, &st.n_chunks);
   if (st.n_chunks > 256) throw CudaError("grid too large: more than 131072 tiles");
   fip::bc_tile_force(cfg, &st.force);
   ck(cudaMalloc((void**)&st.sticky, st.n_tiles), "cudaMalloc");
@@ -281,7 +290,7 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
   }
   ck(cudaMemcpy(d_ctl, h_ctl, sizeof(FipCtl), cudaMemcpyHostToDevice), "cudaMemcpy");
   ck(fip::launch_init_tiles(st, 0, stream), "init_tiles");
-  grid_ctas = fip::rmg_step_grid(device);
+  grid_ctas = fip::rmg_step_grid(device, st.nc);
 
   // boundary-condition program (BoundaryConditionKernel::generate)
   std::string err;
@@ -770,7 +779,7 @@ int fip_restore(fip_handle* h, const char* path) {
     const int k = hd.iteration - 1;
     ck(fip::launch_init_tiles_region(h->st.h[p], h->st.qx[p], h->st.qy[p], h->st.h[p ^ 1], h->st.qx[p ^ 1],
                                      h->st.qy[p ^ 1], h->st.sohle, h->st.W, h->st.H, h->st.pitch, h->st.no_value,
-                                     FIP_TILE_COLS, FIP_TILE_ROWS, h->st.force, h->st.sticky, h->st.nz[k & 1],
+                                     h->st.tile_cols, FIP_TILE_ROWS, h->st.force, h->st.sticky, h->st.nz[k & 1],
                                      h->st.nz[(k + 1) & 1],
                                      h->stream),
        "init_tiles");
