@@ -220,11 +220,12 @@ class Ensemble:
         res = (EnsembleTune * 16)()
         n = ctypes.c_int()
         _lib.check(_lib.lib().fip_ensemble_autotune(self._h, int(steps_per_shape), res, 16, ctypes.byref(n)))
-        return [{"consumer_warps": r.consumer_warps, "tile_cols": r.tile_cols, "tile_rows": r.tile_rows,
-                 "steps": r.steps, "ms_per_step": r.ms_per_step} for r in res[:n.value]]
+        return [{"consumer_warps": r.consumer_warps, "cols_per_thread": r.cols_per_thread, "tile_cols": r.tile_cols,
+                 "tile_rows": r.tile_rows, "steps": r.steps, "ms_per_step": r.ms_per_step} for r in res[:n.value]]
 
-    def set_shape(self, consumer_warps: int, tile_rows: int) -> None:
-        _lib.check(_lib.lib().fip_ensemble_set_shape(self._h, int(consumer_warps), int(tile_rows)))
+    def set_shape(self, consumer_warps: int, tile_rows: int, cols_per_thread: int = 4) -> None:
+        _lib.check(_lib.lib().fip_ensemble_set_shape_nc(self._h, int(consumer_warps), int(tile_rows),
+                                                         int(cols_per_thread)))
 
     def field(self, member: int, name: str = "h") -> np.ndarray:
         H, W = self.shapes[member]

@@ -30,6 +30,7 @@ EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_ru
            "fip_sample", "fip_volume", "fip_get_field", "fip_set_field", "fip_time", "fip_info", "fip_profile_steps", "fip_step_timed", "fip_destroy", "fip_rmg_step_noalloc",
            "fip_last_error", "fip_validate", "fip_config_json", "fip_bc_program",
            "fip_ensemble_init", "fip_ensemble_step", "fip_ensemble_run", "fip_ensemble_autotune", "fip_ensemble_set_shape",
+           "fip_ensemble_set_shape_nc",
            "fip_ensemble_step_timed", "fip_ensemble_get_field", "fip_ensemble_time", "fip_ensemble_info",
            "fip_ensemble_destroy", "fip_checkpoint", "fip_restore", "fip_render", "fip_ensemble_render",
            "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad", "fip_ensemble_gather", "fip_sg_pack_input", "fip_sg_target",
@@ -52,7 +53,7 @@ class FipInfo(ctypes.Structure):
 
 class EnsembleTune(ctypes.Structure):
     _fields_ = [("consumer_warps", ctypes.c_int), ("tile_cols", ctypes.c_int), ("tile_rows", ctypes.c_int),
-                ("steps", ctypes.c_int), ("ms_per_step", ctypes.c_float)]
+                ("steps", ctypes.c_int), ("ms_per_step", ctypes.c_float), ("cols_per_thread", ctypes.c_int)]
 
 
 class EnsembleInfo(ctypes.Structure):
@@ -60,7 +61,7 @@ class EnsembleInfo(ctypes.Structure):
                 ("packed_W", ctypes.c_int), ("packed_rows", ctypes.c_int), ("pitch", ctypes.c_int),
                 ("consumer_warps", ctypes.c_int), ("tile_cols", ctypes.c_int), ("tile_rows", ctypes.c_int),
                 ("n_tiles", ctypes.c_int), ("active_tiles", ctypes.c_int), ("iteration", ctypes.c_int),
-                ("nonfinite", ctypes.c_int)]
+                ("nonfinite", ctypes.c_int), ("cols_per_thread", ctypes.c_int)]
 
 
 class FipError(RuntimeError):
@@ -109,6 +110,7 @@ def lib():
         L.fip_ensemble_run.argtypes = [vp]
         L.fip_ensemble_autotune.argtypes = [vp, ip, ctypes.POINTER(EnsembleTune), ip, ctypes.POINTER(ctypes.c_int)]
         L.fip_ensemble_set_shape.argtypes = [vp, ip, ip]
+        L.fip_ensemble_set_shape_nc.argtypes = [vp, ip, ip, ip]
         L.fip_ensemble_step_timed.argtypes = [vp, ip, fp]
         L.fip_ensemble_get_field.argtypes = [vp, ip, ip, fp]
         L.fip_ensemble_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double), fp, ctypes.POINTER(ctypes.c_int)]
@@ -155,7 +157,8 @@ def lib():
         for name in ("fip_init", "fip_init_ex", "fip_step", "fip_run", "fip_save", "fip_save_current", "fip_sample",
                      "fip_volume", "fip_get_field", "fip_set_field", "fip_time", "fip_info", "fip_profile_steps", "fip_step_timed", "fip_validate",
                      "fip_config_json", "fip_bc_program", "fip_ensemble_init", "fip_ensemble_step", "fip_ensemble_run",
-                     "fip_ensemble_autotune", "fip_ensemble_set_shape", "fip_ensemble_step_timed",
+                     "fip_ensemble_autotune", "fip_ensemble_set_shape", "fip_ensemble_set_shape_nc",
+                     "fip_ensemble_step_timed",
                      "fip_ensemble_get_field", "fip_ensemble_time", "fip_ensemble_info"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L

@@ -66,8 +66,11 @@ constexpr int kGapRows = 3;  // zero rows above, between and below the members
 
 struct Shape {
   int kw, tile_rows;
+  int nc = 4;  // columns per thread
+  int cols() const { return 30 * nc * kw; }
 };
-const Shape kShapes[] = {{4, 32}, {4, 16}, {4, 64}, {2, 32}, {2, 16}, {2, 64}};
+const Shape kShapes[] = {{4, 32, 4}, {4, 16, 4}, {4, 64, 4}, {2, 32, 4}, {2, 16, 4}, {2, 64, 4},
+                         {4, 32, 2}, {4, 16, 2}, {4, 64, 2}};
 
 }  // namespace
 
@@ -229,7 +232,7 @@ void fip_ensemble::init(const std::vector<std::string>& paths, const fip_options
   for (const Shape& s : kShapes) {
     int t = 0;
     for (int m = 0; m < n; ++m)
-      t += ((mem[m].W + 120 * s.kw - 1) / (120 * s.kw)) * ((mem[m].H + s.tile_rows - 1) / s.tile_rows);
+      t += ((mem[m].W + s.cols() - 1) / s.cols()) * ((mem[m].H + s.tile_rows - 1) / s.tile_rows);
     max_tiles = std::max(max_tiles, t);
   }
   max_chunks = (max_tiles + FIP_PLAN_CHUNK - 1) / FIP_PLAN_CHUNK;
@@ -298,7 +301,7 @@ void fip_ensemble::init(const std::vector<std::string>& paths, const fip_options
   std::string err;
   const std::string src = fip::ensemble_post_kernel_source(cp, sers, sbase, mem, pitch);
   if (fip::build_post_kernel(src, &post, &err, "fip_ens_post")) throw std::invalid_argument("NVRTC:" + err);
-  set_shape(Shape{4, 32}, false);
+  set_shape(Shape{4, 32, 4}, false);
   eck(cudaStreamSynchronize(stream), "init");
   (void)paths;
 }
@@ -306,7 +309,7 @@ void fip_ensemble::init(const std::vector<std::string>& paths, const fip_options
 // Tile shape: member table, tile counts, and (replan) the plan of the current state in it.
 void fip_ensemble::set_shape(Shape s, bool replan) {
   shape = s;
-  const int tc = 120 * s.kw;
+  const int tc = s.cols();
   int base = 0;
   for (int m = 0; m < n; ++m) {
     FipEnsMember& M = mem[m];
@@ -320,8 +323,9 @@ void fip_ensemble::set_shape(Shape s, bool replan) {
   st.n_sx = 0;
   st.n_ty = 1;
   st.kw = s.kw;
+  st.nc = s.nc;
   st.tile_rows = s.tile_rows;
-  grid_ctas = fip::rmg_step_grid_kw(device, s.kw);
+  grid_ctas = fip::rmg_step_grid_kw(device, s.kw, s.nc);
   clear_graphs();
   eck(cudaMemcpyAsync(d_mem, mem.data(), sizeof(FipEnsMember) * n, cudaMemcpyHostToDevice, stream), "cudaMemcpy");
   eck(cudaMemsetAsync(st.nz[0], 0, max_tiles, stream), "cudaMemset");
@@ -369,7 +373,7 @@ void fip_ensemble::launch_post(int mode) {
   a.n_members = n;
   a.n_tiles = st.n_tiles;
   a.n_chunks = st.n_chunks;
-  a.tile_cols = 120 * shape.kw;
+  a.tile_cols = shape.cols();
   a.tile_rows = shape.tile_rows;
   a.mode = mode;
   void* params[] = {&a};
@@ -557,8 +561,9 @@ int fip_ensemble_autotune(fip_ensemble* e, int steps_per_shape, fip_ensemble_tun
       const int ran = e->h_ctl->iteration - it0;
       fip_ensemble_tune_t r;
       r.consumer_warps = kShapes[i].kw;
-      r.tile_cols = 120 * kShapes[i].kw;
+      r.tile_cols = kShapes[i].cols();
       r.tile_rows = kShapes[i].tile_rows;
+      r.cols_per_thread = kShapes[i].nc;
       r.steps = ran;
       r.ms_per_step = ran > 0 ? ms / ran : 0.f;
       e->tune.push_back(r);
@@ -578,13 +583,21 @@ int fip_ensemble_autotune(fip_ensemble* e, int steps_per_shape, fip_ensemble_tun
 }
 
 int fip_ensemble_set_shape(fip_ensemble* e, int consumer_warps, int tile_rows) {
+  return fip_ensemble_set_shape_nc(e, consumer_warps, tile_rows, 4);
+}
+
+int fip_ensemble_set_shape_nc(fip_ensemble* e, int consumer_warps, int tile_rows, int cols_per_thread) {
   if (!e) return efail(FIP_ERR_ARG, "null ensemble");
   bool ok = false;
-  for (const Shape& s : kShapes) ok |= (s.kw == consumer_warps && s.tile_rows == tile_rows);
-  if (!ok) return efail(FIP_ERR_ARG, "fip_ensemble_set_shape: consumer_warps must be 2 or 4 and tile_rows 16, 32 or 64");
+  for (const Shape& s : kShapes)
+    ok |= (s.kw == consumer_warps && s.tile_rows == tile_rows && s.nc == cols_per_thread);
+  if (!ok)
+    return efail(FIP_ERR_ARG,
+                 "fip_ensemble_set_shape: consumer_warps must be 2 or 4, tile_rows 16, 32 or 64, and cols_per_thread 4 "
+                 "(or 2 with 4 consumer warps)");
   return eguard([&] {
     eck(cudaSetDevice(e->device), "cudaSetDevice");
-    e->set_shape(Shape{consumer_warps, tile_rows}, e->started);
+    e->set_shape(Shape{consumer_warps, tile_rows, cols_per_thread}, e->started);
     eck(cudaStreamSynchronize(e->stream), "set_shape");
     return FIP_OK;
   });
@@ -708,7 +721,8 @@ int fip_ensemble_info(fip_ensemble* e, fip_ensemble_info_t* out) {
     out->packed_rows = e->total_rows;
     out->pitch = e->pitch;
     out->consumer_warps = e->shape.kw;
-    out->tile_cols = 120 * e->shape.kw;
+    out->cols_per_thread = e->shape.nc;
+    out->tile_cols = e->shape.cols();
     out->tile_rows = e->shape.tile_rows;
     out->n_tiles = e->st.n_tiles;
     out->iteration = e->h_ctl->iteration;

@@ -1262,24 +1262,27 @@ cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t strea
   }
   if (st.n_members > FIP_ENS_MAX_MEMBERS) return cudaErrorInvalidValue;
   // ensemble tile shapes: 2 or 4 consumer warps, 16, 32 or 64 rows
-#define FIP_ENS_LAUNCH(KW_, TR_)                                                                   \
-  if (st.kw == KW_ && st.tile_rows == TR_)                                                         \
-    return st.kst ? launch_step_t<true, true, KW_, TR_, 4>(st, grid, stream)                       \
-                  : launch_step_t<false, true, KW_, TR_, 4>(st, grid, stream);
-  FIP_ENS_LAUNCH(4, 32)
-  FIP_ENS_LAUNCH(4, 16)
-  FIP_ENS_LAUNCH(4, 64)
-  FIP_ENS_LAUNCH(2, 32)
-  FIP_ENS_LAUNCH(2, 16)
-  FIP_ENS_LAUNCH(2, 64)
+#define FIP_ENS_LAUNCH(KW_, TR_, NC_)                                                              \
+  if (st.kw == KW_ && st.tile_rows == TR_ && st.nc == NC_)                                         \
+    return st.kst ? launch_step_t<true, true, KW_, TR_, NC_>(st, grid, stream)                     \
+                  : launch_step_t<false, true, KW_, TR_, NC_>(st, grid, stream);
+  FIP_ENS_LAUNCH(4, 32, 4)
+  FIP_ENS_LAUNCH(4, 16, 4)
+  FIP_ENS_LAUNCH(4, 64, 4)
+  FIP_ENS_LAUNCH(2, 32, 4)
+  FIP_ENS_LAUNCH(2, 16, 4)
+  FIP_ENS_LAUNCH(2, 64, 4)
+  FIP_ENS_LAUNCH(4, 32, 2)
+  FIP_ENS_LAUNCH(4, 16, 2)
+  FIP_ENS_LAUNCH(4, 64, 2)
 #undef FIP_ENS_LAUNCH
   return cudaErrorInvalidValue;
 }
 
-int rmg_step_grid_kw(int device, int kw) {
+int rmg_step_grid_kw(int device, int kw, int nc) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return (kw == 2 ? kMinCtas2 : kMinCtas4) * sms;
+  return (nc == 2 ? kMinCtasNarrow : kw == 2 ? kMinCtas2 : kMinCtas4) * sms;
 }
 
 cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t stream) {

@@ -42,8 +42,8 @@ struct StencilState {
   FipEnsCtl* mctl = nullptr;
   int n_members = 0;
   int tile_rows = FIP_TILE_ROWS;
-  int kw = 4;  // consumer warps per CTA: tiles of 120 * kw columns
-  int nc = 4;  // single grids: columns per thread (4, or 2: narrow threads)
+  int kw = 4;  // consumer warps per CTA: tiles of 30 * nc * kw columns
+  int nc = 4;  // columns per thread (4, or 2: narrow threads)
   int tile_cols = FIP_TILE_COLS;  // single grids: 30 * nc * 4
   TileForce force;  // single grids: tiles the boundary conditions keep active
 };
@@ -73,8 +73,9 @@ cudaError_t launch_init_tiles_region(const float* h, const float* qx, const floa
                                      unsigned char* sticky, unsigned char* nz_cur, unsigned char* nz_prev,
                                      cudaStream_t stream);
 
-// CTAs the step kernel runs with for tiles of kw consumer warps (3 per SM for 4 warps, 5 for 2).
-int rmg_step_grid_kw(int device, int kw);
+// CTAs the step kernel runs with for tiles of kw consumer warps and nc columns per thread (3 per
+// SM for 4 warps, 5 for 2, 4 for narrow threads).
+int rmg_step_grid_kw(int device, int kw, int nc);
 
 // hmax = max(hmax, h[parity]) over the whole grid (the reference's flood_plains_kernel).
 cudaError_t launch_hmax_fold(const StencilState& st, int parity, cudaStream_t stream);

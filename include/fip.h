@@ -231,10 +231,11 @@ int fip_bc_program(const char* yaml_path, int pitch, int compile, char* buf, int
 typedef struct fip_ensemble fip_ensemble;
 
 typedef struct {
-  int consumer_warps;  /* 2 or 4: tiles of 240 or 480 columns */
-  int tile_cols, tile_rows;
+  int consumer_warps;  /* 2 or 4 warps per tile */
+  int tile_cols, tile_rows;  /* tile_cols = 30 * cols_per_thread * consumer_warps */
   int steps;           /* ensemble steps timed in this shape */
   float ms_per_step;   /* device time per ensemble step (CUDA events) */
+  int cols_per_thread; /* 4, or 2 (narrow threads: half the registers, more warps per SM) */
 } fip_ensemble_tune_t;
 
 typedef struct {
@@ -245,6 +246,7 @@ typedef struct {
   int n_tiles, active_tiles;  /* tiles of all members / computed by the next step */
   int iteration;       /* ensemble steps taken */
   int nonfinite;
+  int cols_per_thread;
 } fip_ensemble_info_t;
 
 int fip_ensemble_init(const char* const* yaml_paths, int n_members, const fip_options* opt, fip_ensemble** out);
@@ -257,6 +259,8 @@ int fip_ensemble_run(fip_ensemble* e);
 int fip_ensemble_autotune(fip_ensemble* e, int steps_per_shape, fip_ensemble_tune_t* results, int max_results,
                           int* n_results);
 int fip_ensemble_set_shape(fip_ensemble* e, int consumer_warps, int tile_rows);
+/* The same with the columns per thread (4, or 2 with 4 consumer warps: 240-column tiles). */
+int fip_ensemble_set_shape_nc(fip_ensemble* e, int consumer_warps, int tile_rows, int cols_per_thread);
 /* n_steps ensemble steps timed with CUDA events on the ensemble's stream. */
 int fip_ensemble_step_timed(fip_ensemble* e, int n_steps, float* total_ms);
 /* Member field (FIP_FIELD_H .. FIP_FIELD_TERRAIN) into a W x H host buffer. */

@@ -61,14 +61,17 @@ def test_ensemble_members_match_single_runs(tmp_path):
             _check_member(e, m, ref, rt)
 
 
-@pytest.mark.parametrize("kw,rows", [(4, 32), (4, 16), (4, 64), (2, 32), (2, 16), (2, 64)])
-def test_ensemble_tile_shapes_are_exact(tmp_path, kw, rows):
+@pytest.mark.parametrize("kw,rows,nc", [(4, 32, 4), (4, 16, 4), (4, 64, 4), (2, 32, 4), (2, 16, 4), (2, 64, 4),
+                                        (4, 32, 2), (4, 16, 2), (4, 64, 2)])
+def test_ensemble_tile_shapes_are_exact(tmp_path, kw, rows, nc):
     paths = _members(tmp_path, long=True)[:4]
     K = 120
     with Ensemble(paths) as e:
-        e.set_shape(kw, rows)
+        e.set_shape(kw, rows, nc)
         e.step(K)
-        assert e.info().tile_rows == rows and e.info().consumer_warps == kw
+        inf = e.info()
+        assert inf.tile_rows == rows and inf.consumer_warps == kw and inf.cols_per_thread == nc
+        assert inf.tile_cols == 30 * nc * kw
         for m, p in enumerate(paths):
             ref, rt = _single(p, K)
             _check_member(e, m, ref, rt)
@@ -100,7 +103,7 @@ def test_ensemble_all_tiles_matches(tmp_path):
             _check_member(e, m, ref, rt)
 
 
-@pytest.mark.parametrize("all_tiles,shape", [(True, (4, 32)), (False, (2, 16))])
+@pytest.mark.parametrize("all_tiles,shape", [(True, (4, 32)), (False, (2, 16)), (False, (4, 16, 2))])
 def test_large_ensemble_multi_chunk_members_match_single_runs(tmp_path, all_tiles, shape):
     """Members of 0.5 to 3 M cells whose tiles together fill several 512-tile chunks of the
     concatenated plan (1 131 tiles of 480 x 32, 3 957 of 240 x 16): every member still computes
