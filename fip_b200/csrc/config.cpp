@@ -235,6 +235,11 @@ int load_config(const std::string& path, Config* out, std::string* err, bool qui
     }
     c.qx0 = config["qx"].defined() ? load_grid(config["qx"], c.W, c.H) : std::vector<float>(n, 0.f);
     c.qy0 = config["qy"].defined() ? load_grid(config["qy"], c.W, c.H) : std::vector<float>(n, 0.f);
+    // zeros as +0 (the step writes +0 for every zero discharge and depth it computes, so a dry
+    // tile skipped by the active-tile plan then holds exactly what computing it would give)
+    for (std::vector<float>* g : {&c.h0, &c.qx0, &c.qy0})
+      for (float& v : *g)
+        if (v == 0.f) v = 0.f;
     if (config["kSt_var"].defined()) {
       c.has_kst_var = true;
       c.kst = load_grid(config["kSt_var"], c.W, c.H);

@@ -38,7 +38,10 @@ namespace {
 constexpr float kDH = 0.01f;         // src/kernels.cu:23
 constexpr float kEPS = 10e-7f;       // src/kernels.cu:24 (EPS_TROCKEN)
 constexpr float kG = 9.81f;          // src/simdata.h:358
-constexpr int kNSlotKvar = 6;
+#ifndef FIP_NSLOT_KVAR
+#define FIP_NSLOT_KVAR 6
+#endif
+constexpr int kNSlotKvar = FIP_NSLOT_KVAR;
 constexpr int kNSlotUniform = 7;
 constexpr int kNSlotMax = 10;  // ring depth in rows: 6 with the kSt field, else 7 (leaves L1 room beside 3 CTAs)
 // two-warp tiles (240 columns, used by ensembles when the autotuner picks them): 5 CTAs per SM,
@@ -48,10 +51,7 @@ constexpr int kNSlotUniform2 = 10;
 constexpr int kMinCtas2 = 5;
 constexpr int kMinCtas4 = 3;  // resident CTAs per SM (128 registers per thread)
 // narrow threads (2 columns each, tiles of 240 columns): half the registers, more CTAs per SM
-#ifndef FIP_NARROW_CTAS
-#define FIP_NARROW_CTAS 4
-#endif
-constexpr int kMinCtasNarrow = FIP_NARROW_CTAS;
+constexpr int kMinCtasNarrow = 4;  // 95 registers, no spills (5 per SM spill 128 bytes)
 constexpr int kNSlotKvarNarrow = 7;
 constexpr int kNSlotUniformNarrow = 8;
 constexpr int kMaxChunks = 256;
@@ -203,38 +203,10 @@ __device__ __forceinline__ void vfma(float (&d)[N], float2 a, const float (&b)[N
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
 
-#ifndef FIP_VAR_MAX3
-#define FIP_VAR_MAX3 0
-#endif
-#ifndef FIP_VAR_IK2
-#define FIP_VAR_IK2 0
-#endif
-#ifndef FIP_VAR_POW
-#define FIP_VAR_POW 0
-#endif
-// max(a, b, c) in one instruction (sm_100 three-input max), flush-to-zero like fmaxf under
-// -use_fast_math
-__device__ __forceinline__ float fmax3(float a, float b, float c) {
-#if FIP_VAR_MAX3
-  float r;
-  asm("max.ftz.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-  return r;
-#else
-  return fmaxf(fmaxf(a, b), c);
-#endif
-}
-// (1 / a)^2.33 of the friction factor
-__device__ __forceinline__ float pow_inv(float a) {
-#if FIP_VAR_POW
-  float l, r;
-  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(a));
-  l *= -2.33f;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l));
-  return r;
-#else
-  return powf(1.f / a, 2.33f);
-#endif
-}
+// max(a, b, c) as the reference nests it (max(max(DH, h_i), h_east))
+__device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
+// (1 / a)^2.33 of the friction factor, as the reference writes it (powf of the reciprocal)
+__device__ __forceinline__ float pow_inv(float a) { return powf(1.f / a, 2.33f); }
 
 // The NC staged values of `field` at staged column `col` of a ring slot (one 16- or 8-byte
 // shared-memory load)
@@ -383,7 +355,7 @@ struct StepShape {
   static_assert(X0 >= NC && X0 + TC + NC <= kCols && X0 % 4 == 0, "staged window");
 };
 
-template <bool KVAR, bool ENS, int KW, int TRT, int NC>
+template <bool KVAR, bool ENS, int KW, int TRT, int NC, bool KINV>
 __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
     rmg_step_kernel(const __grid_constant__ CUtensorMap tm_h0, const __grid_constant__ CUtensorMap tm_h1,
                     const __grid_constant__ CUtensorMap tm_qx0, const __grid_constant__ CUtensorMap tm_qx1,
@@ -412,7 +384,9 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
   // ensemble: broadcast operands of the member's packed arithmetic (dt / dx dependent), the same way
   __shared__ __align__(16) float s_mcf[ENS ? KW : 1][12];
 
-  unsigned char* ring = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
+  // 1024-byte aligned ring, addressed from the shared array itself so that its loads compile to
+  // shared-memory loads (an integer round trip of the address would make them generic loads)
+  unsigned char* ring = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
   FipCtl* ctl = a.ctl;
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -692,14 +666,16 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
       if (KVAR) {
         float kk[NC];
         ldsv<NC, kFB>(kk, sl0, F_K, scol);
-#if FIP_VAR_IK2
-        const float g = ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg;  // the field holds 1 / kSt^2
-        vmul(fric, kk, make_float2(g, g));
-#else
-        vmul(kk, kk, kk);
+        if constexpr (KINV) {
+          // the field holds 1 / (kSt * kSt) (prepare_kst_field): (dt * G) / (kSt * kSt) is computed
+          // as (dt * G) * (1 / (kSt * kSt)), which is how the fast division evaluates it
+          const float g = ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg;
+          vmul(fric, kk, make_float2(g, g));
+        } else {
+          vmul(kk, kk, kk);
 #pragma unroll
-        for (int k = 0; k < NC; ++k) fric[k] = (ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg) / kk[k];
-#endif
+          for (int k = 0; k < NC; ++k) fric[k] = (ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg) / kk[k];
+        }
       } else {
 #pragma unroll
         for (int k = 0; k < NC; ++k) fric[k] = ENS ? ldsf_at_use(&s_mcf[warp][10]) : fric_u;
@@ -840,13 +816,15 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
         vadd(t, c_one, rx);
 #pragma unroll
         for (int k = 0; k < NC; ++k) qx2[k] = dsum[k] / t[k];
-        vadd(qx2, qx2, c_zero);
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           float q = fminf(qx2[k], lim0[k]);
           q = fmaxf(q, -(k < NC - 1 ? lim0[k + 1] : limE0));
           qx2[k] = holdX[k] ? qx0[k] : q;  // boundary-face holds (:373-376)
         }
+        // zeros as +0: fp32div_wrapper returns +0 for a zero dividend, and a quiescent tile then
+        // computes exactly the +0 its cells hold (inputs are loaded with +0 for zeros too)
+        vadd(qx2, qx2, c_zero);
         // y: -dgy - dfy - dhy + dhg
         vsub(t, gy1, gy0);
         vmul(dsum, t, c_ndxi);                  // -dgy
@@ -864,13 +842,13 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
         vadd(t, c_one, ry);
 #pragma unroll
         for (int k = 0; k < NC; ++k) qy2[k] = dsum[k] / t[k];
-        vadd(qy2, qy2, c_zero);
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           float q = fminf(qy2[k], lim0[k]);
           q = fmaxf(q, -lim1[k]);
           qy2[k] = hold_y ? qy0[k] : q;
         }
+        vadd(qy2, qy2, c_zero);
       }
       const float qx2W = __shfl_up_sync(0xffffffffu, qx2[NC - 1], 1);
 
@@ -1185,7 +1163,22 @@ int make_tensor_maps(StencilState* st) {
   return 0;
 }
 
-#if FIP_VAR_IK2
+// -0 -> +0 in place (bit test: denormals and every other value stay as they are)
+__global__ void positive_zero_kernel(float* a, int W, int H, int pitch) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  if (c < W && r < H) {
+    const size_t o = (size_t)r * pitch + c;
+    if (__float_as_uint(a[o]) == 0x80000000u) a[o] = 0.f;
+  }
+}
+
+cudaError_t launch_positive_zero(float* a, int W, int H, int pitch, cudaStream_t stream) {
+  if (W <= 0 || H <= 0) return cudaSuccess;
+  positive_zero_kernel<<<dim3((W + 255) / 256, H), 256, 0, stream>>>(a, W, H, pitch);
+  return cudaGetLastError();
+}
+
+// kSt -> 1 / (kSt * kSt) in place, with the same fast reciprocal the step's division uses
 __global__ void kst_inverse_kernel(float* k, int W, int H, int pitch) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
   if (c < W && r < H) {
@@ -1193,16 +1186,11 @@ __global__ void kst_inverse_kernel(float* k, int W, int H, int pitch) {
     k[o] = 1.f / (k[o] * k[o]);
   }
 }
-#endif
 
 cudaError_t prepare_kst_field(float* kst, int W, int H, int pitch, cudaStream_t stream) {
-#if FIP_VAR_IK2
   if (!kst) return cudaSuccess;
   kst_inverse_kernel<<<dim3((W + 255) / 256, H), 256, 0, stream>>>(kst, W, H, pitch);
   return cudaGetLastError();
-#else
-  return cudaSuccess;
-#endif
 }
 
 int rmg_step_grid(int device, int nc) {
@@ -1213,13 +1201,13 @@ int rmg_step_grid(int device, int nc) {
 
 int single_tile_cols(int nc) { return nc == 2 ? StepShape<2, 4>::TC : StepShape<4, 4>::TC; }
 
-template <bool KVAR, bool ENS, int KW, int TRT, int NC>
+template <bool KVAR, bool ENS, int KW, int TRT, int NC, bool KINV = true>
 static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t stream) {
   using S = StepShape<NC, KW>;
   constexpr int NF = KVAR ? 5 : 4;
   const int smem = (KVAR ? S::kNSlotK : S::kNSlotU) * NF * S::kFB + 1024;
   static std::atomic<uint64_t> configured{0};
-  const cudaError_t e = ensure_dynamic_smem(rmg_step_kernel<KVAR, ENS, KW, TRT, NC>, smem, configured);
+  const cudaError_t e = ensure_dynamic_smem(rmg_step_kernel<KVAR, ENS, KW, TRT, NC, KINV>, smem, configured);
   if (e != cudaSuccess) return e;
   StepArgs a;
   for (int b = 0; b < 2; ++b) {
@@ -1245,7 +1233,7 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
   a.members = st.members;
   a.mctl = st.mctl;
   a.n_members = st.n_members;
-  rmg_step_kernel<KVAR, ENS, KW, TRT, NC><<<grid, (KW + 1) * 32, smem, stream>>>(
+  rmg_step_kernel<KVAR, ENS, KW, TRT, NC, KINV><<<grid, (KW + 1) * 32, smem, stream>>>(
       st.tm_h[0], st.tm_h[1], st.tm_qx[0], st.tm_qx[1], st.tm_qy[0], st.tm_qy[1], st.tm_sohle, st.tm_kst, a);
   return cudaGetLastError();
 }
@@ -1254,11 +1242,9 @@ cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t strea
   if (st.n_chunks > kMaxChunks) return cudaErrorInvalidValue;
   constexpr int T = FIP_TILE_ROWS;
   if (!st.members) {
-    if (st.nc == 2)
-      return st.kst ? launch_step_t<true, false, 4, T, 2>(st, grid, stream)
-                    : launch_step_t<false, false, 4, T, 2>(st, grid, stream);
-    return st.kst ? launch_step_t<true, false, 4, T, 4>(st, grid, stream)
-                  : launch_step_t<false, false, 4, T, 4>(st, grid, stream);
+    if (!st.kst) return launch_step_t<false, false, 4, T, 4>(st, grid, stream);
+    return st.kst_raw ? launch_step_t<true, false, 4, T, 4, false>(st, grid, stream)
+                      : launch_step_t<true, false, 4, T, 4, true>(st, grid, stream);
   }
   if (st.n_members > FIP_ENS_MAX_MEMBERS) return cudaErrorInvalidValue;
   // ensemble tile shapes: 2 or 4 consumer warps, 16, 32 or 64 rows
@@ -1466,6 +1452,7 @@ extern "C" int fip_rmg_step_noalloc(const float* h_in, const float* qx_in, const
   st.qy[1] = qy_out;
   st.sohle = const_cast<float*>(terrain);
   st.kst = const_cast<float*>(kst_or_null);
+  st.kst_raw = 1;  // the caller's kSt grid as it is (the kernel divides by kSt * kSt)
   st.hmax = nullptr;
   st.ctl = reinterpret_cast<FipCtl*>(scratch + kNoAllocCtlOff);
   st.sticky = nullptr;

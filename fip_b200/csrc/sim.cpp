@@ -66,12 +66,6 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace fip
 
 namespace {
-// Columns per stencil thread of single grids: 4, or 2 with FIP_STENCIL_NC=2 in the environment
-int stencil_nc() {
-  const char* v = std::getenv("FIP_STENCIL_NC");
-  return (v && v[0] == '2' && v[1] == 0) ? 2 : 4;
-}
-
 // NVTX range for the lifetime of a scope (visible under Nsight Systems / ncu --nvtx; a no-op when
 // no tool is attached)
 struct Range {
@@ -222,7 +216,7 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
   st.dx = cfg.dx;
   st.kst_fixed = cfg.kst_fixed;
   st.no_value = cfg.no_data;
-  st.nc = stencil_nc();
+  st.nc = 4;
   st.tile_cols = fip::single_tile_cols(st.nc);
   fip::tile_geometry(st.W, st.H, st.tile_cols, &st.n_sx, &st.n_ty, &st.n_tiles, &st.n_chunks);
   if (st.n_chunks > 256) throw CudaError("grid too large: more than 131072 tiles");
@@ -863,6 +857,7 @@ int fip_set_field(fip_handle* h, int field, const float* src) {
     float* const* bufs = field == FIP_FIELD_H ? h->st.h : field == FIP_FIELD_QX ? h->st.qx : h->st.qy;
     const size_t W = h->cfg.W, H = h->cfg.H, pb = (size_t)h->st.pitch * 4;
     ck(cudaMemcpy2DAsync(bufs[p], pb, src, W * 4, W * 4, H, cudaMemcpyHostToDevice, h->stream), "fip_set_field");
+    ck(fip::launch_positive_zero(bufs[p], (int)W, (int)H, h->st.pitch, h->stream), "fip_set_field");
     ck(cudaMemcpy2DAsync(bufs[p ^ 1], pb, bufs[p], pb, W * 4, H, cudaMemcpyDeviceToDevice, h->stream),
        "fip_set_field");
     if (field == FIP_FIELD_H && !h->h_ctl->hmax_full) {
@@ -918,7 +913,8 @@ int fip_step_exchange(fip_handle* h, int n_steps, float* h_dst, float* qx_dst, f
       float* const* bufs[3] = {h->st.h, h->st.qx, h->st.qy};
       for (int f = 0; f < 3; ++f) {
         ck(cudaMemcpyAsync(bufs[f][p], x.slot_in[s][f], bytes, cudaMemcpyDeviceToDevice, h->stream), "exchange");
-        ck(cudaMemcpyAsync(bufs[f][p ^ 1], x.slot_in[s][f], bytes, cudaMemcpyDeviceToDevice, h->stream), "exchange");
+        ck(fip::launch_positive_zero(bufs[f][p], (int)h->cfg.W, (int)h->cfg.H, h->st.pitch, h->stream), "exchange");
+        ck(cudaMemcpyAsync(bufs[f][p ^ 1], bufs[f][p], bytes, cudaMemcpyDeviceToDevice, h->stream), "exchange");
       }
       ck(cudaEventRecord(x.in_free[s], h->stream), "exchange");
       // a negative depth makes the hmax fold cover inactive tiles (as fip_set_field); the flag

@@ -245,14 +245,16 @@ def scenario1(outdir: str, W: int = 5667, H: int = 6500, dx: float = 3.0, dt: fl
     init = {}
     if wet_start:
         # flooded start: water up to a level 1.5 m above the 35th terrain percentile (ponds and the
-        # channel), seeded discharges in the wet cells, dry on no_data cells
-        rng_w = np.random.default_rng(seed + 23)
+        # channel), discharges from smooth seeded fields (|u| <= 0.3 m/s) in the wet cells, dry on
+        # no_data cells
         level = float(np.percentile(z[~mask_nd], 35)) + 1.5
         depth = np.clip(level - z, 0.0, 6.0).astype(np.float32)
         depth[mask_nd] = 0.0
         wet = depth > 0
-        qx0 = (0.3 * depth * rng_w.standard_normal((H, W)).astype(np.float32) * wet).astype(np.float32)
-        qy0 = (0.3 * depth * rng_w.standard_normal((H, W)).astype(np.float32) * wet).astype(np.float32)
+        ux = 0.6 * fbm(W, H, 0.9, seed + 23)
+        uy = 0.6 * fbm(W, H, 0.9, seed + 29)
+        qx0 = np.where(wet, depth * ux, 0.0).astype(np.float32)
+        qy0 = np.where(wet, depth * uy, 0.0).astype(np.float32)
         for k, a in (("z", z + depth), ("qx", qx0), ("qy", qy0)):
             path = os.path.join(outdir, f"{name}_{k}0.bin")
             write_grid(path, a.astype(np.float32))
