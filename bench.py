@@ -168,43 +168,65 @@ def make_workload(args, rank):
     return sc
 
 
-def cpu_baseline(sc, seconds: float, steps_hint: int | None = None):
-    """FP64 oracle port, all host threads, on a row band of the scenario around the inflow."""
+def _pitch(W):
+    return ((W * 4 + 511) // 512) * 128  # cudaMallocPitch's 512-byte row alignment, in floats
+
+
+def cpu_baseline(sc, seconds: float):
+    """FP64 oracle port (the restatement of the reference's kernel, boundary conditions and dt
+    control) on the whole scenario: all host threads for about `seconds`, then one thread for a
+    few steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
     threads = os.cpu_count() or 1
-    W, H = sc.W, sc.H
-
-    def band(rows):
-        r0 = max(0, min(H - rows, sc.info["inflow_rows"][0] - rows // 2))
-        sl = slice(r0, r0 + rows)
-        o = pyoracle.Oracle(W, rows, ((W * 4 + 511) // 512) * 128, 3.0, 0.5, True, 30.0, -1.0,
-                            np.ascontiguousarray(sc.terrain[sl]), None, None, None,
-                            np.ascontiguousarray(sc.kst_var[sl]), precision=64)
-        o.set_threads(threads)
-        return o, r0
-
-    o, _ = band(min(H, 256))
+    cells = sc.W * sc.H
+    o = pyoracle.Oracle.from_yaml(sc.yaml_path, _pitch(sc.W), precision=64)
+    o.set_threads(threads)
     t0 = time.perf_counter()
     o.simulate(1)
-    t1 = time.perf_counter() - t0
-    per_row = t1 / min(H, 256)
-    if steps_hint:
-        rows = int(max(64, min(H, seconds / max(steps_hint, 1) / per_row)))
-        n = steps_hint
-    else:
-        rows = min(H, 1024)
-        n = max(2, int(seconds / (per_row * rows)))
-    o, r0 = band(rows)
-    o.simulate(1)
+    per = time.perf_counter() - t0
+    n = max(2, int(seconds / max(per, 1e-6)))
     t0 = time.perf_counter()
     o.simulate(n)
     dt = time.perf_counter() - t0
-    value = W * rows * n / dt
-    return {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"FP64 oracle, rows {r0}-{r0 + rows - 1} of the {W}x{H} scenario (all {W} columns), "
-                      f"{n} steps in {dt:.1f} s, {threads} threads"}, n, dt
+    o.set_threads(1)
+    n1 = max(1, int(min(seconds / 3, 8.0) / max(per * threads, 1e-6)))
+    t0 = time.perf_counter()
+    o.simulate(n1)
+    dt1 = time.perf_counter() - t0
+    return {"value": cells * n / dt, "unit": METRIC, "cores": threads, "kind": "port",
+            "single_thread_value": cells * n1 / dt1,
+            "sample": f"FP64 oracle, whole {sc.W}x{sc.H} scenario with its boundary conditions and variable dt: "
+                      f"{n} steps in {dt:.1f} s on {threads} threads, then {n1} steps in {dt1:.1f} s on 1 thread"}
+
+
+def cpu_baseline_config0():
+    """The 1024 x 1024 plain-solver case over its full 10 000 steps (dt 0.1 s), FP64 oracle port,
+    all host threads; one thread timed on its first 200 steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    from fip_b200 import synth
+
+    d = os.path.join(tempfile.gettempdir(), f"fip_bench_c0_{os.getpid()}")
+    sc = synth.scenario0(d, W=1024, H=1024, dt=0.1, duration=1000.0, save_every=0, name="c0")
+    threads = os.cpu_count() or 1
+    o = pyoracle.Oracle.from_yaml(sc.yaml_path, _pitch(1024), precision=64)
+    o.set_threads(threads)
+    t0 = time.perf_counter()
+    o.run_to(1000.0)
+    dt = time.perf_counter() - t0
+    steps = o.iteration
+    o1 = pyoracle.Oracle.from_yaml(sc.yaml_path, _pitch(1024), precision=64)
+    o1.set_threads(1)
+    t0 = time.perf_counter()
+    o1.simulate(200)
+    dt1 = time.perf_counter() - t0
+    return {"workload": "1024x1024 plain-solver case, dt 0.1 s, 10000 steps", "steps": steps,
+            "wall_s": dt, "cores": threads, "cell_updates_per_s": 1024 * 1024 * steps / dt,
+            "single_thread_cell_updates_per_s": 1024 * 1024 * 200 / dt1,
+            "single_thread_wall_s_extrapolated": dt1 * steps / 200}
 
 
 def gpu_reference_baseline(args, local_rank, duration):
@@ -363,8 +385,7 @@ def run_reference(args, rank, world):
 
     sc = make_workload(args, rank)
     threads = os.cpu_count() or 1
-    pitch = ((sc.W * 4 + 511) // 512) * 128  # cudaMallocPitch's 512-byte row alignment
-    o = pyoracle.Oracle.from_yaml(sc.yaml_path, pitch, precision=64)
+    o = pyoracle.Oracle.from_yaml(sc.yaml_path, _pitch(sc.W), precision=64)
     o.set_threads(threads)
     o.simulate(max(args.warmup, 1))
     t0 = time.perf_counter()
@@ -482,7 +503,9 @@ def run_gpu(args, rank, world, local_rank):
     if rank == 0:
         base = None
         if world == 1 and not args.no_cpu_baseline:
-            base, _, _ = cpu_baseline(sc, args.cpu_seconds)
+            base = cpu_baseline(sc, args.cpu_seconds)
+            if args.cpu_config0:
+                base["config0"] = cpu_baseline_config0()
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -539,6 +562,8 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=8, help="e2e steps (at least; more when --steps is larger)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-config0", action="store_true",
+                    help="also time the oracle port over the full 1024x1024, 10000-step case")
     ap.add_argument("--gpu-ref-seconds", type=float, default=120.0,
                     help="simulated s of the reference-binary baseline on this GPU (0: skip)")
     ap.add_argument("--ens-members", type=int, default=64, help="batched-ensemble measurement (0: skip)")
