@@ -216,7 +216,6 @@ void fip_ensemble::init(const std::vector<std::string>& paths, const fip_options
       // arithmetic in both forms of the kernel
       if (c.has_kst_var) up(st.kst, c.kst);
       else up(st.kst, std::vector<float>(W * H, c.kst_fixed));
-      eck(fip::prepare_kst_field(st.kst + off, (int)W, (int)H, pitch, stream), "kst");
     }
   }
   st.W = packed_W;

@@ -122,6 +122,13 @@ __device__ __forceinline__ void tma_row(void* dst, const CUtensorMap* tm, int x,
       "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
+// L2 prefetch of one 256-float box (no shared memory, no barrier): brings a row that the ring
+// will stage a few rows later from HBM into L2, so that its staging copy is an L2 hit
+__device__ __forceinline__ void tma_prefetch_row(const CUtensorMap* tm, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(tm)),
+               "r"(x), "r"(y)
+               : "memory");
+}
 __device__ __forceinline__ void record_error(FipCtl* ctl, int code) { atomicCAS(&ctl->error, 0, code); }
 // Shared-memory values read where they are used: a volatile load is neither hoisted out of the
 // row loop nor merged with an earlier one, so the value holds no register between its uses.
@@ -203,6 +210,15 @@ __device__ __forceinline__ void vfma(float (&d)[N], float2 a, const float (&b)[N
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
 
+#ifndef FIP_PREFETCH_ROWS
+#define FIP_PREFETCH_ROWS 0
+#endif
+#ifndef FIP_VAR_NOSEL
+#define FIP_VAR_NOSEL 0
+#endif
+#ifndef FIP_VAR_NANMAX
+#define FIP_VAR_NANMAX 0
+#endif
 // max(a, b, c) as the reference nests it (max(max(DH, h_i), h_east))
 __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
 // (1 / a)^2.33 of the friction factor, as the reference writes it (powf of the reciprocal)
@@ -355,7 +371,7 @@ struct StepShape {
   static_assert(X0 >= NC && X0 + TC + NC <= kCols && X0 % 4 == 0, "staged window");
 };
 
-template <bool KVAR, bool ENS, int KW, int TRT, int NC, bool KINV>
+template <bool KVAR, bool ENS, int KW, int TRT, int NC>
 __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
     rmg_step_kernel(const __grid_constant__ CUtensorMap tm_h0, const __grid_constant__ CUtensorMap tm_h1,
                     const __grid_constant__ CUtensorMap tm_qx0, const __grid_constant__ CUtensorMap tm_qx1,
@@ -477,6 +493,19 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
             tma_row(dst + F_S * kFB + 1024 * b, &tm_s, x0 + 256 * b, y, &full_bar[slot]);
             if (KVAR) tma_row(dst + F_K * kFB + 1024 * b, &tm_k, x0 + 256 * b, y, &full_bar[slot]);
           }
+#if FIP_PREFETCH_ROWS > 0
+          if (j + FIP_PREFETCH_ROWS <= rb) {  // rows of this run only (all inside the grid)
+            const int yp = y + FIP_PREFETCH_ROWS;
+#pragma unroll
+            for (int b = 0; b < S::kBoxes; ++b) {
+              tma_prefetch_row(th, x0 + 256 * b, yp);
+              tma_prefetch_row(tqx, x0 + 256 * b, yp);
+              tma_prefetch_row(tqy, x0 + 256 * b, yp);
+              tma_prefetch_row(&tm_s, x0 + 256 * b, yp);
+              if (KVAR) tma_prefetch_row(&tm_k, x0 + 256 * b, yp);
+            }
+          }
+#endif
         }
       }
       // drain: never leave the CTA with copies in flight into its shared memory
@@ -530,7 +559,11 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
   // CFL: dx / (sqrt(G h') + max |u|) is monotone in its denominator, so the minimum over the cells
   // is dx over the largest denominator; the division happens once per warp
   float den_max = 0.0f;
+#if FIP_VAR_NANMAX
+  float nanhi = 0.f, nanlo = 0.f;  // NaN-propagating max / min of the computed depths
+#else
   unsigned expacc = 0u;  // largest exponent field of a computed depth
+#endif
   uint32_t seq = 0;
   Walk w = walk0;
   int s, ra, rb, m = 0;
@@ -666,16 +699,9 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
       if (KVAR) {
         float kk[NC];
         ldsv<NC, kFB>(kk, sl0, F_K, scol);
-        if constexpr (KINV) {
-          // the field holds 1 / (kSt * kSt) (prepare_kst_field): (dt * G) / (kSt * kSt) is computed
-          // as (dt * G) * (1 / (kSt * kSt)), which is how the fast division evaluates it
-          const float g = ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg;
-          vmul(fric, kk, make_float2(g, g));
-        } else {
-          vmul(kk, kk, kk);
+        vmul(kk, kk, kk);
 #pragma unroll
-          for (int k = 0; k < NC; ++k) fric[k] = (ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg) / kk[k];
-        }
+        for (int k = 0; k < NC; ++k) fric[k] = (ENS ? ldsf_at_use(&s_mcf[warp][11]) : dtg) / kk[k];
       } else {
 #pragma unroll
         for (int k = 0; k < NC; ++k) fric[k] = ENS ? ldsf_at_use(&s_mcf[warp][10]) : fric_u;
@@ -782,11 +808,13 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
         }
         vmul(ry, fric, t);
         vmul(ry, ry, u);
+#if !FIP_VAR_NOSEL
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           rx[k] = (mx[k] == 0.f) ? 0.f : rx[k];
           ry[k] = (my[k] == 0.f) ? 0.f : ry[k];
         }
+#endif
       }
       // compute_rmg_qx / compute_rmg_qy (:75-127): the same expression trees; 0.5 G h^2 as
       // nhh = (-0.5 G h) h = -(0.5 G h h)
@@ -881,10 +909,19 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           const bool wk = (mH >> k) & 1;
+#if !FIP_VAR_NANMAX
           expacc = max(expacc, __float_as_uint(h2[k]) & 0x7f800000u);  // all-ones exponent: NaN/Inf
+#endif
           den_max = fmaxf(den_max, (wk && h2[k] > kEPS) ? t[k] : 0.0f);
           nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & 0x7fffffffu;
         }
+#if FIP_VAR_NANMAX
+#pragma unroll
+        for (int k = 0; k < NC; k += 2) {
+          asm("max.NaN.f32 %0, %0, %1, %2;" : "+f"(nanhi) : "f"(h2[k]), "f"(h2[k + 1]));
+          asm("min.NaN.f32 %0, %0, %1, %2;" : "+f"(nanlo) : "f"(h2[k]), "f"(h2[k + 1]));
+        }
+#endif
         const size_t row_off = (size_t)(r + (ENS ? lds_at_use(&s_msc[warp][1]) : 0)) * (size_t)pitch + (size_t)c;
         if (mH == FULL) {
           stgv<NC>(h_out + row_off, h2);
@@ -996,7 +1033,12 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
   // denominator, one atomicMin per warp on the float bits (all positive)
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) den_max = fmaxf(den_max, __shfl_xor_sync(0xffffffffu, den_max, off));
+#if FIP_VAR_NANMAX
+  const bool any_bad = __any_sync(0xffffffffu, (__float_as_uint(nanhi) & 0x7f800000u) == 0x7f800000u ||
+                                                    (__float_as_uint(nanlo) & 0x7f800000u) == 0x7f800000u);
+#else
   const bool any_bad = __any_sync(0xffffffffu, expacc == 0x7f800000u);
+#endif
   if (lane == 0) {
     const float cfl = den_max > 0.0f ? fminf(1.0f, dx / den_max) : 1.0f;
     if (cfl < 1.0f) atomicMin(&ctl->cfl_bits[it & 1], __float_as_uint(cfl));
@@ -1178,20 +1220,7 @@ cudaError_t launch_positive_zero(float* a, int W, int H, int pitch, cudaStream_t
   return cudaGetLastError();
 }
 
-// kSt -> 1 / (kSt * kSt) in place, with the same fast reciprocal the step's division uses
-__global__ void kst_inverse_kernel(float* k, int W, int H, int pitch) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
-  if (c < W && r < H) {
-    const size_t o = (size_t)r * pitch + c;
-    k[o] = 1.f / (k[o] * k[o]);
-  }
-}
 
-cudaError_t prepare_kst_field(float* kst, int W, int H, int pitch, cudaStream_t stream) {
-  if (!kst) return cudaSuccess;
-  kst_inverse_kernel<<<dim3((W + 255) / 256, H), 256, 0, stream>>>(kst, W, H, pitch);
-  return cudaGetLastError();
-}
 
 int rmg_step_grid(int device, int nc) {
   int sms = 148;
@@ -1201,13 +1230,13 @@ int rmg_step_grid(int device, int nc) {
 
 int single_tile_cols(int nc) { return nc == 2 ? StepShape<2, 4>::TC : StepShape<4, 4>::TC; }
 
-template <bool KVAR, bool ENS, int KW, int TRT, int NC, bool KINV = true>
+template <bool KVAR, bool ENS, int KW, int TRT, int NC>
 static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t stream) {
   using S = StepShape<NC, KW>;
   constexpr int NF = KVAR ? 5 : 4;
   const int smem = (KVAR ? S::kNSlotK : S::kNSlotU) * NF * S::kFB + 1024;
   static std::atomic<uint64_t> configured{0};
-  const cudaError_t e = ensure_dynamic_smem(rmg_step_kernel<KVAR, ENS, KW, TRT, NC, KINV>, smem, configured);
+  const cudaError_t e = ensure_dynamic_smem(rmg_step_kernel<KVAR, ENS, KW, TRT, NC>, smem, configured);
   if (e != cudaSuccess) return e;
   StepArgs a;
   for (int b = 0; b < 2; ++b) {
@@ -1233,7 +1262,7 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
   a.members = st.members;
   a.mctl = st.mctl;
   a.n_members = st.n_members;
-  rmg_step_kernel<KVAR, ENS, KW, TRT, NC, KINV><<<grid, (KW + 1) * 32, smem, stream>>>(
+  rmg_step_kernel<KVAR, ENS, KW, TRT, NC><<<grid, (KW + 1) * 32, smem, stream>>>(
       st.tm_h[0], st.tm_h[1], st.tm_qx[0], st.tm_qx[1], st.tm_qy[0], st.tm_qy[1], st.tm_sohle, st.tm_kst, a);
   return cudaGetLastError();
 }
@@ -1241,11 +1270,9 @@ static cudaError_t launch_step_t(const StencilState& st, int grid, cudaStream_t 
 cudaError_t launch_rmg_step(const StencilState& st, int grid, cudaStream_t stream) {
   if (st.n_chunks > kMaxChunks) return cudaErrorInvalidValue;
   constexpr int T = FIP_TILE_ROWS;
-  if (!st.members) {
-    if (!st.kst) return launch_step_t<false, false, 4, T, 4>(st, grid, stream);
-    return st.kst_raw ? launch_step_t<true, false, 4, T, 4, false>(st, grid, stream)
-                      : launch_step_t<true, false, 4, T, 4, true>(st, grid, stream);
-  }
+  if (!st.members)
+    return st.kst ? launch_step_t<true, false, 4, T, 4>(st, grid, stream)
+                  : launch_step_t<false, false, 4, T, 4>(st, grid, stream);
   if (st.n_members > FIP_ENS_MAX_MEMBERS) return cudaErrorInvalidValue;
   // ensemble tile shapes: 2 or 4 consumer warps, 16, 32 or 64 rows
 #define FIP_ENS_LAUNCH(KW_, TR_, NC_)                                                              \
@@ -1452,7 +1479,6 @@ extern "C" int fip_rmg_step_noalloc(const float* h_in, const float* qx_in, const
   st.qy[1] = qy_out;
   st.sohle = const_cast<float*>(terrain);
   st.kst = const_cast<float*>(kst_or_null);
-  st.kst_raw = 1;  // the caller's kSt grid as it is (the kernel divides by kSt * kSt)
   st.hmax = nullptr;
   st.ctl = reinterpret_cast<FipCtl*>(scratch + kNoAllocCtlOff);
   st.sticky = nullptr;

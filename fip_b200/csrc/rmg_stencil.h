@@ -26,8 +26,7 @@ struct StencilState {
   float* qx[2];
   float* qy[2];
   float* sohle;
-  float* kst;   // nullptr: uniform kst_fixed; else 1 / (kSt * kSt) (prepare_kst_field)
-  int kst_raw = 0;  // kst holds kSt itself (callers' grids)
+  float* kst;   // nullptr: uniform kst_fixed
   float* hmax;
   FipCtl* ctl;  // device control block
   unsigned char* sticky;  // per tile: always active (boundary-condition cells, static water on cells the step never writes)
@@ -98,11 +97,6 @@ cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, cons
 // Replaces -0 by +0 in a W x H field of row pitch `pitch` (uploaded states: the step writes +0
 // for every zero it computes, so a quiescent tile must hold +0 for skipping it to be exact).
 cudaError_t launch_positive_zero(float* a, int W, int H, int pitch, cudaStream_t stream);
-
-// Converts an uploaded kSt grid (W x H of row pitch `pitch`) into the form the step kernel reads:
-// 1 / (kSt * kSt), so that the friction coefficient (dt * G) / (kSt * kSt) of every cell and step
-// costs one multiplication instead of a division.
-cudaError_t prepare_kst_field(float* kst, int W, int H, int pitch, cudaStream_t stream);
 
 // Number of CTAs the single-grid step kernel runs with (3 per SM with 4 columns per thread, 5
 // with 2).

@@ -208,7 +208,6 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
   up(st.hmax, cfg.h0);
   up(st.sohle, cfg.terrain);
   if (cfg.has_kst_var) up(st.kst, cfg.kst);
-  if (st.kst) ck(fip::prepare_kst_field(st.kst, (int)W, (int)H, pitch, stream), "kst");
 
   st.W = (int)W;
   st.H = (int)H;
@@ -1170,10 +1169,10 @@ int copy_out(const std::string& s, char* buf, int buflen) {
   return (int)s.size();
 }
 
-int load_for_host(const char* path, fip::Config* c) {
+int load_for_host(const char* path, fip::Config* c, bool quiet) {
   if (!path) return fail(FIP_ERR_ARG, "null path");
   std::string err;
-  const int rc = fip::load_config(path, c, &err);
+  const int rc = fip::load_config(path, c, &err, quiet);
   if (rc == 2) return fail(FIP_ERR_IO, err);
   if (rc) return fail(FIP_ERR_CONFIG, err);
   return FIP_OK;
@@ -1185,12 +1184,12 @@ extern "C" {
 
 int fip_validate(const char* yaml_path) {
   fip::Config c;
-  return load_for_host(yaml_path, &c);
+  return load_for_host(yaml_path, &c, false);  // validation prints the reference's warnings
 }
 
 int fip_config_json(const char* yaml_path, char* buf, int buflen) {
   fip::Config c;
-  int rc = load_for_host(yaml_path, &c);
+  int rc = load_for_host(yaml_path, &c, true);
   if (rc) return rc;
   static const char* sides[] = {"left", "right", "top", "bottom"};
   static const char* types[] = {"z", "q", "close", "open"};
@@ -1234,7 +1233,7 @@ int fip_config_json(const char* yaml_path, char* buf, int buflen) {
 
 int fip_bc_program(const char* yaml_path, int pitch, int compile, char* buf, int buflen) {
   fip::Config c;
-  int rc = load_for_host(yaml_path, &c);
+  int rc = load_for_host(yaml_path, &c, true);
   if (rc) return rc;
   if (pitch < (int)c.W) return fail(FIP_ERR_ARG, "pitch smaller than W");
   fip::SeriesLayout ser = fip::layout_series(c);
