@@ -106,12 +106,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+#ifndef FIP_WAIT_HINT
+#define FIP_WAIT_HINT 0
+#endif
+// try_wait that lets the hardware suspend the thread for up to `ns` nanoseconds (it resumes as
+// soon as the phase completes), so a waiting warp issues no spin instructions meanwhile
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
 // Bounded wait for the phase of `parity` to complete; false after kWaitNs.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t i = 1;; ++i) {
+#if FIP_WAIT_HINT > 0
+    if (mbar_try_wait_sleep(bar, parity, FIP_WAIT_HINT)) return true;
+#else
     if (mbar_try_wait(bar, parity)) return true;
+#endif
     if ((i & 63u) == 0 && globaltimer() - t0 > kWaitNs) return false;
   }
 }
@@ -215,6 +235,12 @@ __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; 
 #endif
 #ifndef FIP_VAR_NOSEL
 #define FIP_VAR_NOSEL 0
+#endif
+#ifndef FIP_VAR_SQRTMAX
+#define FIP_VAR_SQRTMAX 0
+#endif
+#ifndef FIP_VAR_UNROLL2
+#define FIP_VAR_UNROLL2 0
 #endif
 #ifndef FIP_VAR_NANMAX
 #define FIP_VAR_NANMAX 0
@@ -672,6 +698,9 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
     // rows r-1 .. r+2 stay staged during row r: qy(r-1) and the terrain of row r are read
     // again instead of being carried in registers; row r-1 is released at the end of row r
     unsigned nzacc = 0u;
+#if FIP_VAR_UNROLL2
+#pragma unroll 2
+#endif
     for (int r = ra - 1; r < rb; ++r) {
       {  // wait for row r+2
         const bool got = __all_sync(0xffffffffu, mbar_wait(&full_bar[i2], ph2));
@@ -796,19 +825,27 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
         vfma(my, uxy, uxy, t);
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
+#if FIP_VAR_SQRTMAX
+          t[k] = sqrtf(fmaxf(mx[k], 1.17549435e-38f));
+#else
           t[k] = sqrtf(mx[k]);
+#endif
           u[k] = pow_inv(ax1[k]);
         }
         vmul(rx, fric, t);
         vmul(rx, rx, u);
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
+#if FIP_VAR_SQRTMAX
+          t[k] = sqrtf(fmaxf(my[k], 1.17549435e-38f));
+#else
           t[k] = sqrtf(my[k]);
+#endif
           u[k] = pow_inv(ay1[k]);
         }
         vmul(ry, fric, t);
         vmul(ry, ry, u);
-#if !FIP_VAR_NOSEL
+#if !FIP_VAR_NOSEL && !FIP_VAR_SQRTMAX
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           rx[k] = (mx[k] == 0.f) ? 0.f : rx[k];

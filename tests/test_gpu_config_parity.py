@@ -5,12 +5,13 @@
   src/kernels.cu with the wet/dry mask off, deterministic): every dump of depth, qx, qy and flood
   plains within |dz|, |dq| <= 1e-4, identical wet sets, the same step count.
 * The 5667 x 6500 large grid (2448 tiles of 480 x 32 cells: five plan chunks, so the kernels' walk
-  over a multi-chunk active-tile list is exercised) from a flooded start with seeded discharges:
-  - fixed dt, 50 steps, against the FP32 oracle: h, qx, qy, both ping-pong partners and hmax
-    within the gates, identical wet sets; FP64 volume within 1e-6 relative; and the dry-tile
-    skipping run bit-identical to the every-tile run;
-  - variable dt against the reference binary with a synchronised CFL readback
-    (oracle/_ref/fip_ref_sync): the same step count and dumps within the gates.
+  over a multi-chunk active-tile list is exercised) from a flooded start with smooth seeded
+  discharges, fixed dt, 50 steps, against the FP32 oracle: h, qx, qy, both ping-pong partners and
+  hmax within the gates, identical wet sets; FP64 volume within 1e-6 relative; and the dry-tile
+  skipping run bit-identical to the every-tile run.
+* The 5667 x 6500 grid as specified (dry start), variable dt, against the reference binary with a
+  synchronised CFL readback (oracle/_ref/fip_ref_sync): the same step count and dumps within the
+  gates.
 The reference binaries are built from the reference's sources by oracle/ref.mk; tests that need
 them are skipped (with the reason) where they were not built.
 """
@@ -118,12 +119,13 @@ def test_config1_full_grid_fixed_dt_matches_oracle(tmp_path):
 
 
 def test_config1_full_grid_variable_dt_matches_reference_binary(tmp_path):
-    """5667 x 6500 flooded start, variable dt from 0.1 s for 20 simulated s: the reference with a
+    """5667 x 6500 as specified (dry start, q inflow hydrograph, open bottom, kSt_var, no_data
+    border), variable dt, the first 300 simulated s (about 600 steps): the reference with a
     synchronised CFL readback against fip_run (same step count, dumps within the gates)."""
     _need("fip_ref_sync")
-    from fip_b200 import Simulation
+    from fip_b200 import Simulation, synth
 
-    mk = lambda d: _flood1(d, variable_dt=True, duration=20.0, save_state=["10", "20"])
+    mk = lambda d: synth.scenario1(d, duration=300.0, name="cfg1", save_state=["150", "300"])
     sref, sours = _two_copies(tmp_path, mk)
     r = refbin.run("fip_ref_sync", sref.yaml_path)
     with Simulation(sours.yaml_path, quiet=True) as sim:
