@@ -35,7 +35,7 @@ EXPORTS = ("fip_default_options", "fip_init", "fip_init_ex", "fip_step", "fip_ru
            "fip_ensemble_destroy", "fip_checkpoint", "fip_restore", "fip_render", "fip_ensemble_render",
            "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad", "fip_ensemble_gather", "fip_sg_pack_input", "fip_sg_target",
            "fip_sg_loss", "fip_sg_bias_grad", "fip_sg_adamw", "fip_sg_cast_weights", "fip_sg_apply",
-           "fip_sg_edge_flux", "fip_sg_consistency", "fip_sg_pin", "fip_sg_edges", "fip_inject_wait_timeout",
+           "fip_sg_edge_flux", "fip_sg_consistency", "fip_sg_level_bound", "fip_sg_pin", "fip_sg_edges", "fip_inject_wait_timeout",
            "fip_stage_state",
            "fip_step_exchange", "fip_exchange_wait")
 
@@ -134,13 +134,14 @@ def lib():
         L.fip_sg_apply.argtypes = [vp, ip, ip, ip, f32, vp, f32, vp, vp, vp, vp, vp, vp]
         L.fip_sg_edge_flux.argtypes = [vp, vp, ip, ip, ip, vp, vp]
         L.fip_sg_consistency.argtypes = [vp, ip, ip, ip, f32, vp, f32, vp, vp, vp, vp]
+        L.fip_sg_level_bound.argtypes = [vp, vp, vp, vp, vp, ip, ip, ip, f32, ip, f32, vp, vp, vp]
         L.fip_sg_pin.argtypes = [vp, vp, vp, vp, ll, vp, vp, vp, vp]
         L.fip_sg_pin.restype = ctypes.c_int
         L.fip_sg_edges.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, ip, f32, vp]
         L.fip_sg_edges.restype = ctypes.c_int
         for name in ("fip_ensemble_gather", "fip_sg_conv3x3", "fip_sg_conv3x3_wgrad", "fip_sg_pack_input",
                      "fip_sg_target", "fip_sg_loss", "fip_sg_bias_grad", "fip_sg_adamw", "fip_sg_cast_weights",
-                     "fip_sg_apply", "fip_sg_edge_flux", "fip_sg_consistency"):
+                     "fip_sg_apply", "fip_sg_edge_flux", "fip_sg_consistency", "fip_sg_level_bound"):
             getattr(L, name).restype = ctypes.c_int
         L.fip_inject_wait_timeout.argtypes = [vp]
         L.fip_inject_wait_timeout.restype = ctypes.c_int

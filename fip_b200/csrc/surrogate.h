@@ -66,6 +66,8 @@ cudaError_t cast_weights(const float* p, int n_layers, __nv_bfloat16* wf, __nv_b
 cudaError_t apply_update(const float* pred, int N, int H, int W, float dx, const float* terr, float no_value, float* h,
                          float* qx, float* qy, double* dvol, float* hmax, cudaStream_t s);
 cudaError_t edge_flux(const float* qx, const float* qy, int N, int H, int W, double* flux, cudaStream_t s);
+cudaError_t level_bound(float* h, float* qx, float* qy, const float* terr, const float* zcap, int N, int H, int W,
+                        float no_value, int clip, float umax, double* excess, float* hmax, cudaStream_t s);
 cudaError_t consistency(const float* pred, int N, int H, int W, float dx, const float* terr, float no_value,
                         const float* qx, const float* qy, double* res, cudaStream_t s);
 cudaError_t edge_cells(float* h, const float* terr, int N, int H, int W, const int* types, float no_value,

@@ -133,6 +133,14 @@ int fip_sg_apply(const float* pred, int N, int H, int W, float dx, const float* 
   return sg_cuda(fip::sg::apply_update(pred, N, H, W, dx, terrain, no_value, h, qx, qy, dvol, hmax, SG_S), "fip_sg_apply");
 }
 
+int fip_sg_level_bound(float* h, float* qx, float* qy, const float* terrain, const float* zcap, int N, int H, int W,
+                       float no_value, int clip, float umax, double* excess, float* hmax, void* stream) {
+  if (!h || !qx || !qy || !terrain || !zcap || !excess || N <= 0 || (long long)H * W < 256 || !(umax >= 0.f))
+    return sg_fail(FIP_ERR_ARG, "fip_sg_level_bound: bad argument (images of at least 256 cells)");
+  return sg_cuda(fip::sg::level_bound(h, qx, qy, terrain, zcap, N, H, W, no_value, clip, umax, excess, hmax, SG_S),
+                 "fip_sg_level_bound");
+}
+
 int fip_sg_consistency(const float* pred, int N, int H, int W, float dx, const float* terrain, float no_value,
                        const float* qx, const float* qy, double* res, void* stream) {
   if (!pred || !terrain || !qx || !qy || !res || N <= 0 || (long long)H * W < 256 || H < 3 || W < 4 || !(dx > 0.f))

@@ -281,6 +281,59 @@ __global__ void consistency_kernel(const float* __restrict__ pred, int N, int H,
   }
 }
 
+// Level bound of one call, after the update: in the surrogate's scenarios the water comes from
+// a level condition, so no water surface may rise above that level (plus a margin): every cell
+// whose level h + terrain exceeds zcap[n] holds water that the network made up. excess[n] +=
+// the sum of those depths above the bound (a depth sum: times dx^2 a volume); with `clip` the
+// depth is cut back to the bound and the discharges to |q| <= umax * h; hmax (optional) folds
+// the resulting depth.
+__global__ void level_bound_kernel(float* __restrict__ h, float* __restrict__ qx, float* __restrict__ qy,
+                                   const float* __restrict__ terr, const float* __restrict__ zcap, int N, int H,
+                                   int W, float no_value, int clip, float umax, double* __restrict__ excess,
+                                   float* __restrict__ hmax) {
+  __shared__ double red[2][256];
+  __shared__ int s_n0;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t total = (size_t)N * H * W;
+  const size_t img = (size_t)H * W;
+  double ex = 0.0;
+  int n = 0;
+  if (i < total) {
+    n = (int)(i / img);
+    if (terr[i] != no_value) {
+      const float cap = fmaxf(0.f, zcap[n] - terr[i]);
+      float d = h[i];
+      if (d > cap) {
+        ex = (double)d - (double)cap;
+        if (clip) h[i] = d = cap;
+      }
+      if (clip) {
+        const float qm = umax * fmaxf(d, 0.f);
+        qx[i] = fminf(fmaxf(qx[i], -qm), qm);
+        qy[i] = fminf(fmaxf(qy[i], -qm), qm);
+      }
+      if (hmax) hmax[i] = fmaxf(hmax[i], d);
+    }
+  }
+  if (threadIdx.x == 0) s_n0 = (int)(((size_t)blockIdx.x * blockDim.x) / img);
+  __syncthreads();
+  const int slot = n - s_n0;
+  red[0][threadIdx.x] = (i < total && slot == 0) ? ex : 0.0;
+  red[1][threadIdx.x] = (i < total && slot == 1) ? ex : 0.0;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + s];
+      red[1][threadIdx.x] += red[1][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(&excess[s_n0], red[0][0]);
+    if (s_n0 + 1 < N && red[1][0] != 0.0) atomicAdd(&excess[s_n0 + 1], red[1][0]);
+  }
+}
+
 // Net discharge into the inner cells [2, W-2] x [1, H-2] per image (qx sits on east faces,
 // qy on north faces): + qx[y][1] - qx[y][W-2] over rows 1..H-2, + qy[0][x] - qy[H-2][x] over
 // columns 2..W-2 (a sum of discharges per unit width; times dx gives m3/s).
@@ -414,6 +467,14 @@ cudaError_t consistency(const float* pred, int N, int H, int W, float dx, const 
   const size_t total = (size_t)N * H * W;
   consistency_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(pred, N, H, W, kCallS / dx * kOutF, terr,
                                                                       no_value, qx, qy, res);
+  return cudaGetLastError();
+}
+
+cudaError_t level_bound(float* h, float* qx, float* qy, const float* terr, const float* zcap, int N, int H, int W,
+                        float no_value, int clip, float umax, double* excess, float* hmax, cudaStream_t s) {
+  const size_t total = (size_t)N * H * W;
+  level_bound_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(h, qx, qy, terr, zcap, N, H, W, no_value, clip,
+                                                                      umax, excess, hmax);
   return cudaGetLastError();
 }
 

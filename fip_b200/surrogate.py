@@ -197,11 +197,14 @@ class Surrogate:
         self.cast()
 
     # ---- one surrogate call ------------------------------------------------------------------
-    def advance(self, state, pins=None, hmax=None, resid=None):
+    def advance(self, state, pins=None, hmax=None, resid=None, bound=None):
         """state: dict of device tensors h, qx, qy, terrain, kst [N][H][W], zref [N], no_value;
         h/qx/qy advance by 60 s in place (hmax, if given, folds the new depths; resid, a device
-        double [N], accumulates the call's consistency residual, fip_sg_consistency). Returns the
-        per-image depth-sum change of the inner cells (device double [N])."""
+        double [N], accumulates the call's consistency residual, fip_sg_consistency). bound =
+        (zcap [N], excess [N] double, umax): the level bound of fip_sg_level_bound is applied to
+        the new state (depths above zcap cut back, |q| <= umax h) and the depth it removed is
+        added to excess. Returns the per-image depth-sum change of the inner cells (device double
+        [N])."""
         h, qx, qy = state["h"], state["qx"], state["qy"]
         N, H, W = h.shape
         self.pack(h, qx, qy, state["terrain"], state["kst"], state["zref"], state["no_value"], N, H, W)
@@ -211,9 +214,15 @@ class Surrogate:
                                                  _ptr(state["terrain"]), float(state["no_value"]), _ptr(qx),
                                                  _ptr(qy), _ptr(resid), _stream()))
         dvol = self.torch.zeros(N, dtype=self.torch.float64, device=self.dev)
+        fold_in_apply = hmax is not None and bound is None
         _lib.check(self.L.fip_sg_apply(_ptr(pred), N, H, W, float(state.get("dx", 3.0)), _ptr(state["terrain"]),
                                        float(state["no_value"]), _ptr(h), _ptr(qx), _ptr(qy), _ptr(dvol),
-                                       _ptr(hmax) if hmax is not None else None, _stream()))
+                                       _ptr(hmax) if fold_in_apply else None, _stream()))
+        if bound is not None:
+            zcap, excess, umax = bound
+            _lib.check(self.L.fip_sg_level_bound(_ptr(h), _ptr(qx), _ptr(qy), _ptr(state["terrain"]), _ptr(zcap), N, H,
+                                                 W, float(state["no_value"]), 1, float(umax), _ptr(excess),
+                                                 _ptr(hmax) if hmax is not None else None, _stream()))
         sides = state.get("sides")
         if sides is not None:  # (left, right, top, bottom): 0 none, 1 close, 2 open
             _lib.check(self.L.fip_sg_edges(_ptr(h), _ptr(state["terrain"]), N, H, W, *[int(t) for t in sides],

@@ -32,6 +32,8 @@ from . import Ensemble, synth
 from .surrogate import Surrogate
 
 CALL_S = 60.0
+LEVEL_MARGIN = 0.25  # m above the inflow level that a surrogate water surface may reach
+UMAX = 10.0          # m/s: |q| <= UMAX * h after each surrogate call
 DT = 0.1
 STEPS_PER_CALL = int(round(CALL_S / DT))
 
@@ -80,6 +82,9 @@ class Batch:
                      "qx": torch.zeros_like(self.terrain), "qy": torch.zeros_like(self.terrain)}
         self.no_value = -9999.0
         self.cells = self.n * self.H * self.W
+        # level bound of the rollouts: the inflow level of each member plus LEVEL_MARGIN
+        self.zcap = torch.tensor([float(s.info["zbc"]) + LEVEL_MARGIN for s in scenarios], dtype=torch.float32,
+                                 device=dev)
 
     # edge types of the generator's scenarios (left z is pinned; right open; top and bottom close)
     SIDES = (0, 2, 1, 1)
@@ -219,36 +224,42 @@ def evaluate_one_call(net: Surrogate, batch: Batch, snaps):
 def rollout(net: Surrogate, batch: Batch, n_calls: int, h0, qx0, qy0, residual_threshold: float = 1e-3):
     """Closed-loop surrogate run from (h0, qx0, qy0) over n_calls calls: final state, max-depth
     maps (over the 60-s states) and, per member, whether the fallback indicator tripped and its
-    worst value. The indicator of a call is the network's consistency residual (fip_sg_consistency:
-    the volume on which its face-discharge and discharge-change outputs disagree) relative to the
-    member's water volume (inner cells, floor 1 cm over 1 % of them); it trips above
-    `residual_threshold` (1e-3 of the patch volume) at any call. The mass-balance residual of
-    the state (change of inner volume against 60 s x the mean edge inflow) is reported beside it."""
+    worst value. The water of these scenarios comes from a level condition, so no surface may
+    rise above that level: after every call the depth above the member's inflow level plus
+    LEVEL_MARGIN is removed (and |q| <= UMAX h), and the removed volume -- water the network made
+    up -- relative to the member's water volume (inner cells, floor 1 cm over 1 % of them) is the
+    mass residual that trips the fallback above `residual_threshold` (1e-3 of the patch volume)
+    at any call. The network's consistency residual (fip_sg_consistency) and the mass balance
+    against the edge discharges are reported beside it."""
     torch = _torch()
     st = {"h": h0.clone(), "qx": qx0.clone(), "qy": qy0.clone()}
     state = batch.state(st["h"], st["qx"], st["qy"])
     net.pin(state, batch.pins)  # the iteration-0 boundary conditions
     hmax = st["h"].clone()
     worst = np.zeros(batch.n)
+    worst_cons = np.zeros(batch.n)
     worst_mass = np.zeros(batch.n)
     dx = 3.0
     h_host = st["h"].cpu().numpy()
     vol = h_host[:, 1:-1, 2:-1].astype(np.float64).sum(axis=(1, 2))
     floor = 0.01 * 0.01 * (batch.H - 2) * (batch.W - 3)
     resid = torch.zeros(batch.n, dtype=torch.float64, device=net.dev)
+    excess = torch.zeros(batch.n, dtype=torch.float64, device=net.dev)
     for c in range(n_calls):
         f0 = net.edge_flux(st["qx"], st["qy"])
         resid.zero_()
-        dvol = net.advance(state, batch.pins, hmax, resid=resid)
+        excess.zero_()
+        dvol = net.advance(state, batch.pins, hmax, resid=resid, bound=(batch.zcap, excess, UMAX))
         f1 = net.edge_flux(st["qx"], st["qy"])
-        dv, a, b, r = dvol.cpu().numpy(), f0.cpu().numpy(), f1.cpu().numpy(), resid.cpu().numpy()
-        vol = vol + dv
-        denom = np.maximum(vol, floor)
-        worst = np.maximum(worst, r / denom)
+        dv, a, b, r, ex = (t.cpu().numpy() for t in (dvol, f0, f1, resid, excess))
+        denom = np.maximum(vol + dv, floor)
+        worst = np.maximum(worst, ex / denom)
+        worst_cons = np.maximum(worst_cons, r / denom)
         worst_mass = np.maximum(worst_mass, np.abs(dv - CALL_S / dx * 0.5 * (a + b)) / denom)
+        vol = vol + dv - ex  # the limiter's removal (mostly inner cells) leaves the patch
     torch.cuda.synchronize()
     tripped = worst > residual_threshold
-    return st, hmax, tripped, worst, worst_mass
+    return st, hmax, tripped, worst, worst_mass, worst_cons
 
 
 def screen(net: Surrogate, sc, hours: float, chunk: int = 32, top_frac: float = 0.1, threshold: float = 1e-3):
@@ -273,14 +284,16 @@ def screen(net: Surrogate, sc, hours: float, chunk: int = 32, top_frac: float = 
     tripped = np.zeros(n, bool)
     worst = np.zeros(n)
     worst_mass = np.zeros(n)
+    worst_cons = np.zeros(n)
     for c0 in range(0, n, chunk):
         part = sc[c0:c0 + chunk]
         bsc = Batch(part)
         h0 = torch.zeros((bsc.n, H, W), dtype=torch.float32, device="cuda")
         q0 = torch.zeros_like(h0)
-        _, hm, tr, wo, wm = rollout(net, bsc, n_sc, h0, q0, q0.clone(), residual_threshold=threshold)
+        _, hm, tr, wo, wm, wc = rollout(net, bsc, n_sc, h0, q0, q0.clone(), residual_threshold=threshold)
         s_hmax[c0:c0 + bsc.n].copy_(hm)
         tripped[c0:c0 + bsc.n], worst[c0:c0 + bsc.n], worst_mass[c0:c0 + bsc.n] = tr, wo, wm
+        worst_cons[c0:c0 + bsc.n] = wc
         del bsc, hm
     t_surrogate = time.perf_counter() - t0
     area = (s_hmax.cpu().numpy() > 0.05).sum(axis=(1, 2))
@@ -299,6 +312,20 @@ def screen(net: Surrogate, sc, hours: float, chunk: int = 32, top_frac: float = 
     t_rerun = time.perf_counter() - t0
     fin, ref, sur = final.cpu().numpy(), ref_hmax.cpu().numpy(), s_hmax.cpu().numpy()
     t_screen = t_surrogate + t_rerun
+    err = np.sqrt(((sur - ref) ** 2).mean(axis=(1, 2)))
+    # the same screen at other thresholds: a re-run member gives exactly the solver's map (the
+    # solver is deterministic and the members independent), its cost taken as its share of the
+    # all-member solver time
+    sweep = []
+    for thr in (1e-4, 1e-3, 1e-2, 1e-1):
+        rr = set(np.argsort(-area)[:k].tolist()) | set(np.nonzero(worst > thr)[0].tolist())
+        f2 = sur.copy()
+        for i in rr:
+            f2[i] = ref[i]
+        t2 = t_surrogate + t_solver_all * len(rr) / n
+        sweep.append({"threshold": thr, "rerun": len(rr), "tripped": int((worst > thr).sum()),
+                      "rmse_hmax_m": _rmse(f2, ref), "iou_5cm": float(np.mean([_iou(f2[i], ref[i]) for i in range(n)])),
+                      "est_wall_s": round(t2, 2), "est_speedup": round(t_solver_all / t2, 3)})
     return {"members": n, "size": [H, W], "hours": hours, "rerun": len(rerun), "top_fraction": top_frac,
             "fallback_tripped": int(tripped.sum()), "fallback_threshold": threshold,
             "indicator_median": float(np.median(worst)), "indicator_max": float(np.max(worst)),
@@ -309,7 +336,11 @@ def screen(net: Surrogate, sc, hours: float, chunk: int = 32, top_frac: float = 
             "rmse_hmax_m": _rmse(fin, ref), "iou_5cm": float(np.mean([_iou(fin[i], ref[i]) for i in range(n)])),
             "rmse_hmax_surrogate_only_m": _rmse(sur, ref),
             "iou_5cm_surrogate_only": float(np.mean([_iou(sur[i], ref[i]) for i in range(n)])),
-            "indicator_vs_error_spearman": _spearman(worst, np.sqrt(((sur - ref) ** 2).mean(axis=(1, 2))))}
+            "indicator_vs_error_spearman": _spearman(worst, err),
+            "consistency_residual_median": float(np.median(worst_cons)),
+            "consistency_vs_error_spearman": _spearman(worst_cons, err),
+            "hmax_rmse_per_member_m_quantiles": [float(np.quantile(err, q)) for q in (0.1, 0.5, 0.9)],
+            "threshold_sweep": sweep}
 
 
 def _spearman(a, b):
@@ -369,8 +400,8 @@ def main(argv=None, emit: bool = True):
         esn, ehmax, _ = solver_trajectories(ev, n_calls)
         res["eval_one_call"] = evaluate_one_call(net, bev, esn)
         res["eval_trace"] = rollout_trace(net, bev, esn)
-        st, hm, tripped, worst, worst_mass = rollout(net, bev, n_calls, esn["h"][0], esn["qx"][0], esn["qy"][0],
-                                                     residual_threshold=a.threshold)
+        st, hm, tripped, worst, worst_mass, worst_cons = rollout(net, bev, n_calls, esn["h"][0], esn["qx"][0],
+                                                                 esn["qy"][0], residual_threshold=a.threshold)
         ref_h = esn["h"][n_calls].cpu().numpy()
         got_h = st["h"].cpu().numpy()
         pers = esn["h"][0].cpu().numpy()
@@ -384,6 +415,7 @@ def main(argv=None, emit: bool = True):
                                "fallback_tripped": int(tripped.sum()), "indicator": worst.tolist(),
                                "hmax_rmse_per_member_m": err.tolist(),
                                "indicator_vs_error_spearman": _spearman(worst, err),
+                               "consistency_residual": worst_cons.tolist(),
                                "mass_balance_residual": worst_mass.tolist()}
         del esn
         torch.cuda.empty_cache()

@@ -70,6 +70,13 @@ int fip_sg_cast_weights(const float* p, int n_layers, void* wf, void* wd, void* 
  * (H * W >= 256); hmax (may be NULL) = max(hmax, new h). */
 int fip_sg_apply(const float* pred, int N, int H, int W, float dx, const float* terrain, float no_value, float* h,
                  float* qx, float* qy, double* dvol, float* hmax, void* stream);
+/* Level bound of a surrogate state (after fip_sg_apply): where the water level h + terrain of
+ * image n exceeds zcap[n] (the highest level its boundary conditions impose, plus a margin),
+ * excess[n] += the depth above the bound (a depth sum, H * W >= 256); with clip != 0 the depth is
+ * cut back to the bound and qx, qy to |q| <= umax * h; hmax (may be NULL) = max(hmax, depth).
+ * No-data cells are skipped. */
+int fip_sg_level_bound(float* h, float* qx, float* qy, const float* terrain, const float* zcap, int N, int H, int W,
+                       float no_value, int clip, float umax, double* excess, float* hmax, void* stream);
 /* Fallback indicator of one call, evaluated before fip_sg_apply: res[n] += sum over the inner
  * cells of image n (H * W >= 256) of |dh_F - dh_q|, the disagreement between the depth change
  * the face-discharge outputs imply (continuity) and the one the discharge-change outputs imply

@@ -107,3 +107,19 @@ def consistency(pred, qx, qy, terrain, no_value, dx=3.0):
     inner[1:H - 1, 2:W - 1] = True
     m = inner[None] & (terrain != no_value)
     return np.array([np.abs(dhf[n] - dhq[n])[m[n]].sum() for n in range(N)])
+
+
+def level_bound(h, qx, qy, terrain, zcap, no_value, umax):
+    """fip_sg_level_bound with clip and hmax: returns (h, qx, qy, excess[N], hmax-fold of the new
+    depth over zeros). Depth above zcap[n] - terrain (at least 0) is removed and summed; then
+    |q| <= umax * h; no-data cells untouched."""
+    h, qx, qy = h.astype(np.float32).copy(), qx.astype(np.float32).copy(), qy.astype(np.float32).copy()
+    valid = terrain != no_value
+    cap = np.maximum(np.float32(0), zcap.astype(np.float32)[:, None, None] - terrain).astype(np.float32)
+    over = valid & (h > cap)
+    excess = np.where(over, h.astype(np.float64) - cap.astype(np.float64), 0.0).sum(axis=(1, 2))
+    h = np.where(over, cap, h).astype(np.float32)
+    qm = (np.float32(umax) * np.maximum(h, np.float32(0))).astype(np.float32)
+    qx = np.where(valid, np.minimum(np.maximum(qx, -qm), qm), qx).astype(np.float32)
+    qy = np.where(valid, np.minimum(np.maximum(qy, -qm), qm), qy).astype(np.float32)
+    return h, qx, qy, excess

@@ -24,7 +24,7 @@ def test_trained_network_beats_persistence(tmp_path):
     esn, _, _ = sr.solver_trajectories(ev, 20)
     one = sr.evaluate_one_call(net, bev, esn)
     assert one["rmse_depth_net_m"] < 0.95 * one["rmse_depth_persistence_m"], one
-    st, _, _, _, _ = sr.rollout(net, bev, 5, esn["h"][0], esn["qx"][0], esn["qy"][0])
+    st, _, _, _, _, _ = sr.rollout(net, bev, 5, esn["h"][0], esn["qx"][0], esn["qy"][0])
     ref = esn["h"][5].cpu().numpy().astype(np.float64)
     got = st["h"].cpu().numpy()
     pers = esn["h"][0].cpu().numpy()

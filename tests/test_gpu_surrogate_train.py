@@ -116,3 +116,30 @@ def test_consistency_indicator_matches_oracle():
     ref = so.consistency(pred[:, 8:-8, 8:-8].astype(np.float64), qx, qy, terr, -9999.0)
     got = res.cpu().numpy()
     assert np.allclose(got, ref, rtol=1e-5), (got, ref)
+
+
+def test_level_bound_matches_oracle():
+    """fip_sg_level_bound (the rollout limiter and mass residual) against its restatement."""
+    import ctypes
+
+    from fip_b200 import _lib
+
+    N, H, W = 3, 33, 41
+    rng = np.random.default_rng(7)
+    terr = rng.uniform(0.0, 3.0, (N, H, W)).astype(np.float32)
+    terr[2, 5:8, 9:12] = -9999.0
+    h = rng.uniform(0.0, 4.0, (N, H, W)).astype(np.float32)
+    qx = (rng.standard_normal((N, H, W)) * 20).astype(np.float32)
+    qy = (rng.standard_normal((N, H, W)) * 20).astype(np.float32)
+    zcap = np.array([3.5, 2.0, 4.2], np.float32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    th, tqx, tqy, tt, tz = dev(h), dev(qx), dev(qy), dev(terr), dev(zcap)
+    ex = torch.zeros(N, dtype=torch.float64, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = _lib.lib().fip_sg_level_bound(p(th), p(tqx), p(tqy), p(tt), p(tz), N, H, W, -9999.0, 1, 10.0, p(ex), None,
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, _lib.last_error()
+    rh, rqx, rqy, rex = so.level_bound(h, qx, qy, terr, zcap, -9999.0, 10.0)
+    assert np.array_equal(th.cpu().numpy(), rh)
+    assert np.array_equal(tqx.cpu().numpy(), rqx) and np.array_equal(tqy.cpu().numpy(), rqy)
+    assert np.allclose(ex.cpu().numpy(), rex, rtol=1e-9)
