@@ -38,10 +38,7 @@ namespace {
 constexpr float kDH = 0.01f;         // src/kernels.cu:23
 constexpr float kEPS = 10e-7f;       // src/kernels.cu:24 (EPS_TROCKEN)
 constexpr float kG = 9.81f;          // src/simdata.h:358
-#ifndef FIP_NSLOT_KVAR
-#define FIP_NSLOT_KVAR 6
-#endif
-constexpr int kNSlotKvar = FIP_NSLOT_KVAR;
+constexpr int kNSlotKvar = 6;
 constexpr int kNSlotUniform = 7;
 constexpr int kNSlotMax = 10;  // ring depth in rows: 6 with the kSt field, else 7 (leaves L1 room beside 3 CTAs)
 // two-warp tiles (240 columns, used by ensembles when the autotuner picks them): 5 CTAs per SM,
@@ -106,32 +103,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-#ifndef FIP_WAIT_HINT
-#define FIP_WAIT_HINT 0
-#endif
-// try_wait that lets the hardware suspend the thread for up to `ns` nanoseconds (it resumes as
-// soon as the phase completes), so a waiting warp issues no spin instructions meanwhile
-__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t ns) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
-      : "memory");
-  return ok != 0;
-}
 // Bounded wait for the phase of `parity` to complete; false after kWaitNs.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t i = 1;; ++i) {
-#if FIP_WAIT_HINT > 0
-    if (mbar_try_wait_sleep(bar, parity, FIP_WAIT_HINT)) return true;
-#else
     if (mbar_try_wait(bar, parity)) return true;
-#endif
     if ((i & 63u) == 0 && globaltimer() - t0 > kWaitNs) return false;
   }
 }
@@ -141,13 +118,6 @@ __device__ __forceinline__ void tma_row(void* dst, const CUtensorMap* tm, int x,
           smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
-}
-// L2 prefetch of one 256-float box (no shared memory, no barrier): brings a row that the ring
-// will stage a few rows later from HBM into L2, so that its staging copy is an L2 hit
-__device__ __forceinline__ void tma_prefetch_row(const CUtensorMap* tm, int x, int y) {
-  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(tm)),
-               "r"(x), "r"(y)
-               : "memory");
 }
 __device__ __forceinline__ void record_error(FipCtl* ctl, int code) { atomicCAS(&ctl->error, 0, code); }
 // Shared-memory values read where they are used: a volatile load is neither hoisted out of the
@@ -230,20 +200,8 @@ __device__ __forceinline__ void vfma(float (&d)[N], float2 a, const float (&b)[N
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
 
-#ifndef FIP_PREFETCH_ROWS
-#define FIP_PREFETCH_ROWS 0
-#endif
-#ifndef FIP_VAR_NOSEL
-#define FIP_VAR_NOSEL 0
-#endif
 #ifndef FIP_VAR_SQRTMAX
 #define FIP_VAR_SQRTMAX 0
-#endif
-#ifndef FIP_VAR_UNROLL2
-#define FIP_VAR_UNROLL2 0
-#endif
-#ifndef FIP_VAR_NANMAX
-#define FIP_VAR_NANMAX 0
 #endif
 // max(a, b, c) as the reference nests it (max(max(DH, h_i), h_east))
 __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
@@ -519,19 +477,6 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
             tma_row(dst + F_S * kFB + 1024 * b, &tm_s, x0 + 256 * b, y, &full_bar[slot]);
             if (KVAR) tma_row(dst + F_K * kFB + 1024 * b, &tm_k, x0 + 256 * b, y, &full_bar[slot]);
           }
-#if FIP_PREFETCH_ROWS > 0
-          if (j + FIP_PREFETCH_ROWS <= rb) {  // rows of this run only (all inside the grid)
-            const int yp = y + FIP_PREFETCH_ROWS;
-#pragma unroll
-            for (int b = 0; b < S::kBoxes; ++b) {
-              tma_prefetch_row(th, x0 + 256 * b, yp);
-              tma_prefetch_row(tqx, x0 + 256 * b, yp);
-              tma_prefetch_row(tqy, x0 + 256 * b, yp);
-              tma_prefetch_row(&tm_s, x0 + 256 * b, yp);
-              if (KVAR) tma_prefetch_row(&tm_k, x0 + 256 * b, yp);
-            }
-          }
-#endif
         }
       }
       // drain: never leave the CTA with copies in flight into its shared memory
@@ -585,11 +530,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
   // CFL: dx / (sqrt(G h') + max |u|) is monotone in its denominator, so the minimum over the cells
   // is dx over the largest denominator; the division happens once per warp
   float den_max = 0.0f;
-#if FIP_VAR_NANMAX
-  float nanhi = 0.f, nanlo = 0.f;  // NaN-propagating max / min of the computed depths
-#else
   unsigned expacc = 0u;  // largest exponent field of a computed depth
-#endif
   uint32_t seq = 0;
   Walk w = walk0;
   int s, ra, rb, m = 0;
@@ -698,9 +639,6 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
     // rows r-1 .. r+2 stay staged during row r: qy(r-1) and the terrain of row r are read
     // again instead of being carried in registers; row r-1 is released at the end of row r
     unsigned nzacc = 0u;
-#if FIP_VAR_UNROLL2
-#pragma unroll 2
-#endif
     for (int r = ra - 1; r < rb; ++r) {
       {  // wait for row r+2
         const bool got = __all_sync(0xffffffffu, mbar_wait(&full_bar[i2], ph2));
@@ -845,7 +783,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
         }
         vmul(ry, fric, t);
         vmul(ry, ry, u);
-#if !FIP_VAR_NOSEL && !FIP_VAR_SQRTMAX
+#if !FIP_VAR_SQRTMAX
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           rx[k] = (mx[k] == 0.f) ? 0.f : rx[k];
@@ -946,19 +884,10 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           const bool wk = (mH >> k) & 1;
-#if !FIP_VAR_NANMAX
           expacc = max(expacc, __float_as_uint(h2[k]) & 0x7f800000u);  // all-ones exponent: NaN/Inf
-#endif
           den_max = fmaxf(den_max, (wk && h2[k] > kEPS) ? t[k] : 0.0f);
           nzacc |= (__float_as_uint(h2[k]) | __float_as_uint(qx2[k]) | __float_as_uint(qy2[k])) & 0x7fffffffu;
         }
-#if FIP_VAR_NANMAX
-#pragma unroll
-        for (int k = 0; k < NC; k += 2) {
-          asm("max.NaN.f32 %0, %0, %1, %2;" : "+f"(nanhi) : "f"(h2[k]), "f"(h2[k + 1]));
-          asm("min.NaN.f32 %0, %0, %1, %2;" : "+f"(nanlo) : "f"(h2[k]), "f"(h2[k + 1]));
-        }
-#endif
         const size_t row_off = (size_t)(r + (ENS ? lds_at_use(&s_msc[warp][1]) : 0)) * (size_t)pitch + (size_t)c;
         if (mH == FULL) {
           stgv<NC>(h_out + row_off, h2);
@@ -1070,12 +999,7 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
   // denominator, one atomicMin per warp on the float bits (all positive)
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) den_max = fmaxf(den_max, __shfl_xor_sync(0xffffffffu, den_max, off));
-#if FIP_VAR_NANMAX
-  const bool any_bad = __any_sync(0xffffffffu, (__float_as_uint(nanhi) & 0x7f800000u) == 0x7f800000u ||
-                                                    (__float_as_uint(nanlo) & 0x7f800000u) == 0x7f800000u);
-#else
   const bool any_bad = __any_sync(0xffffffffu, expacc == 0x7f800000u);
-#endif
   if (lane == 0) {
     const float cfl = den_max > 0.0f ? fminf(1.0f, dx / den_max) : 1.0f;
     if (cfl < 1.0f) atomicMin(&ctl->cfl_bits[it & 1], __float_as_uint(cfl));
