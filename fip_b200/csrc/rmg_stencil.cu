@@ -200,9 +200,6 @@ __device__ __forceinline__ void vfma(float (&d)[N], float2 a, const float (&b)[N
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
 
-#ifndef FIP_VAR_SQRTMAX
-#define FIP_VAR_SQRTMAX 0
-#endif
 // max(a, b, c) as the reference nests it (max(max(DH, h_i), h_east))
 __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
 // (1 / a)^2.33 of the friction factor, as the reference writes it (powf of the reciprocal)
@@ -763,33 +760,23 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
         vfma(my, uxy, uxy, t);
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
-#if FIP_VAR_SQRTMAX
-          t[k] = sqrtf(fmaxf(mx[k], 1.17549435e-38f));
-#else
           t[k] = sqrtf(mx[k]);
-#endif
           u[k] = pow_inv(ax1[k]);
         }
         vmul(rx, fric, t);
         vmul(rx, rx, u);
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
-#if FIP_VAR_SQRTMAX
-          t[k] = sqrtf(fmaxf(my[k], 1.17549435e-38f));
-#else
           t[k] = sqrtf(my[k]);
-#endif
           u[k] = pow_inv(ay1[k]);
         }
         vmul(ry, fric, t);
         vmul(ry, ry, u);
-#if !FIP_VAR_SQRTMAX
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
           rx[k] = (mx[k] == 0.f) ? 0.f : rx[k];
           ry[k] = (my[k] == 0.f) ? 0.f : ry[k];
         }
-#endif
       }
       // compute_rmg_qx / compute_rmg_qy (:75-127): the same expression trees; 0.5 G h^2 as
       // nhh = (-0.5 G h) h = -(0.5 G h h)
