@@ -526,25 +526,48 @@ def run_gpu(args, rank, world, local_rank):
 
 def time_to_solution(args):
     """The large-grid scenario over its whole duration (24 simulated hours, variable dt, dry-tile
-    skipping) through fip_run, and optionally the reference binary (wet/dry mask on) on the same
-    parameter file: wall seconds and steps. Prints one JSON object (not a bench line)."""
+    skipping) through fip_run, and optionally reference binaries (oracle/_ref) on the same
+    parameter file: wall seconds and steps, and the final save_state dumps compared (flood
+    plains and depth). Prints one JSON object (not a bench line)."""
     from fip_b200 import Simulation, synth
 
-    d = os.path.join(tempfile.gettempdir(), f"fip_tts_{os.getpid()}")
-    sc = synth.scenario1(d, W=args.W, H=args.H, seed=1, duration=args.tts_hours * 3600.0, name="tts")
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refbin
+
+    dur = args.tts_hours * 3600.0
+    base = os.path.join(tempfile.gettempdir(), f"fip_tts_{os.getpid()}")
+
+    def scenario(tag):
+        return synth.scenario1(os.path.join(base, tag), W=args.W, H=args.H, seed=1, duration=dur, name="tts",
+                               save_state=[f"{dur:g}"])
+
+    sc = scenario("ours")
     out = {"workload": f"scenario1 {sc.W}x{sc.H}, {args.tts_hours:g} simulated hours, variable dt"}
     with Simulation(sc.yaml_path, quiet=True) as sim:
         t0 = time.perf_counter()
         sim.run()
-        out["fip_b200"] = {"wall_s": time.perf_counter() - t0, "steps": sim.iteration,
-                           "final_dt": sim.time()[1], "active_tile_fraction_end": sim.info().active_tiles / sim.info().n_tiles}
-    if args.tts_reference:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import refbin
-
-        r = refbin.run("fip_ref", sc.yaml_path, timeout=7200)
-        out["reference_fip_ref"] = {"seconds": r["seconds"], "steps": r["iterations"]}
-        out["speedup"] = r["seconds"] / out["fip_b200"]["wall_s"]
+        wall = time.perf_counter() - t0
+        inf = sim.info()
+        out["fip_b200"] = {"wall_s": wall, "steps": sim.iteration, "s_per_step": wall / sim.iteration,
+                           "final_dt": sim.time()[1], "active_tile_fraction_end": inf.active_tiles / inf.n_tiles}
+    ours = refbin.dumps(os.path.join(base, "ours", "tts"))
+    for name in [x for x in args.tts_reference.split(",") if x]:
+        sr = scenario(name)
+        r = refbin.run(name, sr.yaml_path, timeout=7200)
+        o = {"seconds": r["seconds"], "steps": r["iterations"], "s_per_step": r["seconds"] / r["iterations"],
+             "speedup_wall": r["seconds"] / wall}
+        ref = refbin.dumps(os.path.join(base, name, "tts"))
+        for kind in ("flood_plains", "ah"):
+            key = [k for k in ref if k[0] == kind]
+            if key and key[0] in ours:
+                a_, b_ = ref[key[0]].astype(np.float64), ours[key[0]].astype(np.float64)
+                d = np.abs(a_ - b_)
+                wa, wb = a_ > 0.05, b_ > 0.05
+                u = np.logical_or(wa, wb).sum()
+                o[kind] = {"max_abs_diff": float(d.max()), "rmse": float(np.sqrt((d ** 2).mean())),
+                           "cells_over_1e-4": float((d > 1e-4).mean()),
+                           "extent_iou_5cm": float(np.logical_and(wa, wb).sum() / u) if u else 1.0}
+        out[name] = o
     print(json.dumps(out), flush=True)
     return 0
 
@@ -577,7 +600,8 @@ def main():
     ap.add_argument("--sg-batch", type=int, default=16)
     ap.add_argument("--tts", action="store_true", help="only the time-to-solution run of the large grid")
     ap.add_argument("--tts-hours", type=float, default=24.0)
-    ap.add_argument("--tts-reference", action="store_true", help="also run the reference binary for --tts")
+    ap.add_argument("--tts-reference", default="",
+                    help="comma-separated reference binaries (oracle/_ref) to run for --tts, e.g. fip_ref_sync")
     args = ap.parse_args()
     if args.tts:
         return time_to_solution(args)

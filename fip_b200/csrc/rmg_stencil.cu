@@ -1153,18 +1153,43 @@ int make_tensor_maps(StencilState* st) {
   return 0;
 }
 
-// -0 -> +0 in place (bit test: denormals and every other value stay as they are)
-__global__ void positive_zero_kernel(float* a, int W, int H, int pitch) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
-  if (c < W && r < H) {
-    const size_t o = (size_t)r * pitch + c;
-    if (__float_as_uint(a[o]) == 0x80000000u) a[o] = 0.f;
+// -0 -> +0 (bit test: denormals and every other value stay as they are)
+__device__ __forceinline__ float positive_zero(float v) { return __float_as_uint(v) == 0x80000000u ? 0.f : v; }
+
+// dst0 (and dst1 unless null) = src with -0 -> +0, over the W x H cells of row pitch `pitch`
+// (a multiple of 4 floats, 16-byte aligned rows): four cells per thread, the row's last partial
+// group cell by cell. src may be dst0.
+__global__ void positive_zero_copy_kernel(const float* src, float* dst0, float* dst1, int W, int H, int pitch) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  const int c = 4 * g;
+  if (r >= H || c >= W) return;
+  const size_t o = (size_t)r * pitch + c;
+  if (c + 4 <= W) {
+    float4 v = *reinterpret_cast<const float4*>(src + o);
+    v.x = positive_zero(v.x);
+    v.y = positive_zero(v.y);
+    v.z = positive_zero(v.z);
+    v.w = positive_zero(v.w);
+    *reinterpret_cast<float4*>(dst0 + o) = v;
+    if (dst1) *reinterpret_cast<float4*>(dst1 + o) = v;
+  } else {
+    for (int k = 0; k < W - c; ++k) {
+      const float v = positive_zero(src[o + k]);
+      dst0[o + k] = v;
+      if (dst1) dst1[o + k] = v;
+    }
   }
 }
 
 cudaError_t launch_positive_zero(float* a, int W, int H, int pitch, cudaStream_t stream) {
+  return launch_positive_zero_copy(a, a, nullptr, W, H, pitch, stream);
+}
+
+cudaError_t launch_positive_zero_copy(const float* src, float* dst0, float* dst1, int W, int H, int pitch,
+                                      cudaStream_t stream) {
   if (W <= 0 || H <= 0) return cudaSuccess;
-  positive_zero_kernel<<<dim3((W + 255) / 256, H), 256, 0, stream>>>(a, W, H, pitch);
+  const int groups = (W + 3) / 4;
+  positive_zero_copy_kernel<<<dim3((groups + 255) / 256, H), 256, 0, stream>>>(src, dst0, dst1, W, H, pitch);
   return cudaGetLastError();
 }
 

@@ -97,6 +97,9 @@ cudaError_t launch_sample_gather(const StencilState& st, int parity, int n, cons
 // Replaces -0 by +0 in a W x H field of row pitch `pitch` (uploaded states: the step writes +0
 // for every zero it computes, so a quiescent tile must hold +0 for skipping it to be exact).
 cudaError_t launch_positive_zero(float* a, int W, int H, int pitch, cudaStream_t stream);
+// dst0 (and dst1 unless null) = src with -0 -> +0, same geometry (src may be dst0).
+cudaError_t launch_positive_zero_copy(const float* src, float* dst0, float* dst1, int W, int H, int pitch,
+                                      cudaStream_t stream);
 
 // Number of CTAs the single-grid step kernel runs with (3 per SM with 4 columns per thread, 5
 // with 2).

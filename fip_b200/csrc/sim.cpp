@@ -856,8 +856,7 @@ int fip_set_field(fip_handle* h, int field, const float* src) {
     float* const* bufs = field == FIP_FIELD_H ? h->st.h : field == FIP_FIELD_QX ? h->st.qx : h->st.qy;
     const size_t W = h->cfg.W, H = h->cfg.H, pb = (size_t)h->st.pitch * 4;
     ck(cudaMemcpy2DAsync(bufs[p], pb, src, W * 4, W * 4, H, cudaMemcpyHostToDevice, h->stream), "fip_set_field");
-    ck(fip::launch_positive_zero(bufs[p], (int)W, (int)H, h->st.pitch, h->stream), "fip_set_field");
-    ck(cudaMemcpy2DAsync(bufs[p ^ 1], pb, bufs[p], pb, W * 4, H, cudaMemcpyDeviceToDevice, h->stream),
+    ck(fip::launch_positive_zero_copy(bufs[p], bufs[p], bufs[p ^ 1], (int)W, (int)H, h->st.pitch, h->stream),
        "fip_set_field");
     if (field == FIP_FIELD_H && !h->h_ctl->hmax_full) {
       // a negative depth anywhere makes the hmax fold cover inactive tiles too; the check runs on
@@ -910,11 +909,10 @@ int fip_step_exchange(fip_handle* h, int n_steps, float* h_dst, float* qx_dst, f
       const int p = h->h_ctl->parity;
       ck(cudaStreamWaitEvent(h->stream, x.in_ready[s], 0), "fip_step_exchange");
       float* const* bufs[3] = {h->st.h, h->st.qx, h->st.qy};
-      for (int f = 0; f < 3; ++f) {
-        ck(cudaMemcpyAsync(bufs[f][p], x.slot_in[s][f], bytes, cudaMemcpyDeviceToDevice, h->stream), "exchange");
-        ck(fip::launch_positive_zero(bufs[f][p], (int)h->cfg.W, (int)h->cfg.H, h->st.pitch, h->stream), "exchange");
-        ck(cudaMemcpyAsync(bufs[f][p ^ 1], bufs[f][p], bytes, cudaMemcpyDeviceToDevice, h->stream), "exchange");
-      }
+      for (int f = 0; f < 3; ++f)  // one pass: slot -> both ping-pong buffers, zeros as +0
+        ck(fip::launch_positive_zero_copy(x.slot_in[s][f], bufs[f][p], bufs[f][p ^ 1], (int)h->cfg.W, (int)h->cfg.H,
+                                          h->st.pitch, h->stream),
+           "exchange");
       ck(cudaEventRecord(x.in_free[s], h->stream), "exchange");
       // a negative depth makes the hmax fold cover inactive tiles (as fip_set_field); the flag
       // stays on the device, where the stencil reads it
