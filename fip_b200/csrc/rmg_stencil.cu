@@ -750,33 +750,33 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
       for (int k = 0; k < NC; ++k) t[k] = (t[k] + (k > 0 ? qx0[k - 1] : qxW0)) + (k > 0 ? qx1[k - 1] : qxW1);
       vmul(uxy, t, c_q);
       // friction factors fric * sqrt(ux^2 + uy^2) * (1 / a1)^2.33 (:91-94, :118-121), 0 where both
-      // discharges vanish (then the square sum is 0 and the product is 0 for every finite fric)
+      // discharges vanish (then the square sum is 0 and the product is 0 for every finite fric).
+      // x first, then y: each square sum is dead once its factor is selected (fewer live registers)
       float rx[NC], ry[NC];
       {
-        float mx[NC], my[NC];
+        float m2[NC];
         vmul(t, uyx, uyx);
-        vfma(mx, qx0, qx0, t);
-        vmul(t, qy0, qy0);
-        vfma(my, uxy, uxy, t);
+        vfma(m2, qx0, qx0, t);
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
-          t[k] = sqrtf(mx[k]);
+          t[k] = sqrtf(m2[k]);
           u[k] = pow_inv(ax1[k]);
         }
         vmul(rx, fric, t);
         vmul(rx, rx, u);
 #pragma unroll
+        for (int k = 0; k < NC; ++k) rx[k] = (m2[k] == 0.f) ? 0.f : rx[k];
+        vmul(t, qy0, qy0);
+        vfma(m2, uxy, uxy, t);
+#pragma unroll
         for (int k = 0; k < NC; ++k) {
-          t[k] = sqrtf(my[k]);
+          t[k] = sqrtf(m2[k]);
           u[k] = pow_inv(ay1[k]);
         }
         vmul(ry, fric, t);
         vmul(ry, ry, u);
 #pragma unroll
-        for (int k = 0; k < NC; ++k) {
-          rx[k] = (mx[k] == 0.f) ? 0.f : rx[k];
-          ry[k] = (my[k] == 0.f) ? 0.f : ry[k];
-        }
+        for (int k = 0; k < NC; ++k) ry[k] = (m2[k] == 0.f) ? 0.f : ry[k];
       }
       // compute_rmg_qx / compute_rmg_qy (:75-127): the same expression trees; 0.5 G h^2 as
       // nhh = (-0.5 G h) h = -(0.5 G h h)

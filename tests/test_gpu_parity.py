@@ -75,8 +75,9 @@ def test_matches_reference_binary(name, tmp_path):
 
 
 def random_case(tmp, W, H, seed, bcs=None, kst_var=True, no_data=True, dt=0.02, variable_dt=False,
-                name="rnd"):
-    """Wet start with random velocities, terrain relief, kSt_var, no_data holes."""
+                name="rnd", kst_zero=0.0):
+    """Wet start with random velocities, terrain relief, kSt_var (a fraction kst_zero of it 0:
+    infinite friction), no_data holes."""
     from fip_b200 import synth
 
     rng = np.random.default_rng(seed)
@@ -101,6 +102,8 @@ def random_case(tmp, W, H, seed, bcs=None, kst_var=True, no_data=True, dt=0.02, 
            "duration": 1000, "variable_dt": variable_dt}
     if kst_var:
         k = np.where(rng.random((H, W)) < 0.4, 25.0, 40.0).astype(np.float32)
+        if kst_zero:
+            k[rng.random((H, W)) < kst_zero] = 0.0
         files["kst"] = str(tmp / f"{name}_kst.bin")
         synth.write_grid(files["kst"], k)
         cfg["kSt_var"] = [files["kst"], 0]
@@ -145,6 +148,25 @@ def test_matches_oracle_random_state(W, H, steps, tmp_path):
     assert abs(vol - o.volume()) <= 1e-6 * abs(o.volume())
     worst, ok = _close(o.field(pyoracle.F_H), got["h"], atol=2e-2, rtol=0)
     assert ok, f"fp64 h: max |d| = {worst}"
+
+
+def test_infinite_friction_matches_oracle(tmp_path):
+    """kSt_var with zeros (5% of the cells): dt G / kSt^2 is infinite there, the reference's
+    select gives a friction factor of 0 where both discharges vanish and an infinite one (the
+    discharge becomes 0) elsewhere. Against the FP32 oracle."""
+    W, H, steps = 300, 70, 120
+    y = random_case(tmp_path, W, H, seed=41, kst_zero=0.05)
+    sim = _sim(y, quiet=True)
+    sim.step(steps)
+    got = {k: sim.field(k) for k, _ in FIELDS}
+    pitch = sim.pitch
+    sim.close()
+    o = pyoracle.Oracle.from_yaml(y, pitch, precision=32)
+    o.simulate(steps)
+    for k, which in FIELDS:
+        worst, ok = _close(o.field(which), got[k], atol=1e-4, rtol=1e-5)
+        assert ok, f"fp32 {k}: max |d| = {worst}"
+    assert np.array_equal(o.field(pyoracle.F_H) > 1e-6, got["h"] > 1e-6)
 
 
 def test_pitch_scaled_open_outflow(tmp_path):
