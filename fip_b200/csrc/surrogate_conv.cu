@@ -15,8 +15,10 @@
 // tcgen05.mma (kind::f16, bf16 inputs, fp32 accumulation in tensor memory) and commits to
 // mbarriers, and four epilogue warps read the accumulator with tcgen05.ld and apply the fused
 // epilogue (bias, residual, ReLU, ReLU-mask of the backward pass, zero border). Persistent CTAs
-// (one per SM) double-buffer the accumulator so the epilogue of a tile overlaps the MMAs of
-// the next. Every mbarrier wait is bounded; on expiry the kernel records an error, stops and
+// (one per SM) double-buffer the accumulators so the epilogue of a work unit overlaps the MMAs of
+// the next. A work unit is 1 to 3 adjacent 128-pixel tiles whose MMAs are issued interleaved into
+// independent accumulators (measured: the tensor pipe is busy 62% of the time with one tile per
+// unit, 76% with two); how many depends on the epilogue (tiles_per_unit). Every mbarrier wait is bounded; on expiry the kernel records an error, stops and
 // frees its tensor memory.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -39,6 +41,28 @@ constexpr int kWBytes = 9 * kTapBytes;  // 72 KB
 // one slab per kernel row: a tile's 128 rows plus the 2 * dilation rows its dx shifts reach
 constexpr int kSlabStride = 18 * 1024;  // slabs start on 1024-byte boundaries (swizzle pattern); <= 144 rows
 constexpr int kStages = 6;
+// multi-tile form: TP > 1 adjacent 128-pixel tiles per work unit, their MMAs interleaved into TP
+// independent accumulators; a slab of TP * 128 + 2 dil rows (dil <= 8) comes as 136-row TMA boxes
+constexpr int kBoxRows = 136;  // 17 KB, a multiple of 1024 bytes (the swizzle pattern)
+// Tiles per work unit by epilogue, measured on 32 x 512 x 512 (ms per convolution, TP = 1 / 2 / 3):
+// bias+ReLU 0.92 / 0.77 / 0.74, bias+residual+ReLU 0.95 / 0.94 / 0.97, head 0.97 / 0.82 / 0.70,
+// mask 1.03 / 0.93 / 0.95, residual+mask 1.20 / 1.31 / 1.68, plain 0.98 / 0.83 / 0.73. More
+// interleaved accumulators keep the tensor pipe busier; epilogues that load the residual or the
+// mask per pixel are bound by those loads, and more pixels per unit lengthen them.
+template <int EPI>
+constexpr int tiles_per_unit() {
+  return EPI == EPI_RES_MASK ? 1 : (EPI == EPI_BIAS_RES_RELU || EPI == EPI_MASK) ? 2 : 3;
+}
+template <int TP>
+struct FwdShape {
+  static constexpr int kBoxes = TP == 1 ? 1 : (TP * BM + 2 * kMaxDil + kBoxRows - 1) / kBoxRows;
+  static constexpr int kStg = TP == 1 ? kStages : (TP == 2 ? 4 : 3);
+  static constexpr int kStride = TP == 1 ? kSlabStride : kBoxes * kBoxRows * C * 2;
+  static constexpr uint32_t kTmemCols = TP == 1 ? 128u : (TP == 2 ? 256u : 512u);  // two buffers of TP accumulators
+  static constexpr int kSmem = kWBytes + kStg * kStride + 1024;
+  static_assert(kSmem + 512 <= 232448, "shared memory (dynamic + about 400 bytes static)");
+  static_assert(2 * TP * 64 <= (int)kTmemCols, "tensor memory");
+};
 constexpr int kThreads = 192;           // warp 0: TMA, warp 1: MMA + TMEM owner, warps 2-5: epilogue
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
@@ -165,13 +189,17 @@ struct FwdArgs {
 // ---------------------------------------------------------------------------------------------
 // forward / dgrad: out = epilogue(conv3x3(in, weights)) over every padded pixel
 // ---------------------------------------------------------------------------------------------
-template <int EPI>
+// TP: 128-pixel tiles per work unit (1, or 2: the pair form)
+template <int EPI, int TP>
 __global__ void __launch_bounds__(kThreads, 1)
     conv3x3_kernel(const __grid_constant__ CUtensorMap tm_act, const __grid_constant__ CUtensorMap tm_w, FwdArgs a) {
+  using FS = FwdShape<TP>;
+  constexpr int kStages = FS::kStg;
+  constexpr int kSlabStride = FS::kStride;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* s_w = smem;                    // 9 taps x 8 KB
-  unsigned char* s_a = smem + kWBytes;          // kStages x 18 KB: one 136-row slab per dy
+  unsigned char* s_a = smem + kWBytes;          // kStages slabs, one per dy
   __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], w_bar, acc_full[2], acc_empty[2], done_bar;
   __shared__ uint32_t s_tmem;
   __shared__ float s_bias[C];
@@ -193,9 +221,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (tid < C) s_bias[tid] = a.bias ? a.bias[tid] : 0.f;
-  if (warp == 1) {  // two 64-column fp32 accumulators
+  if (warp == 1) {  // two buffers of TP 64-column fp32 accumulators
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                 "r"(128u)
+                 "r"(FS::kTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -212,7 +240,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t it = 0;
       bool ok = true;
       for (int tile = blockIdx.x; ok && tile < a.n_tiles; tile += gridDim.x) {
-        const int p0 = tile * BM;
+        const int p0 = tile * BM * TP;
         for (int r = 0; r < 3; ++r, ++it) {  // rows from p0 + dil * (dy * Wp - 1) serve the taps (dy, -1..1)
           const uint32_t st = it % kStages, ph = (it / kStages) & 1u;
           if (!mbar_wait(&empty_bar[st], ph ^ 1u, &s_abort)) {
@@ -222,8 +250,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           const int dy = r - 1;
-          mbar_expect_tx(&full_bar[st], (uint32_t)a.slab_rows * C * 2);
-          tma_2d(s_a + st * kSlabStride, &tm_act, 0, p0 + a.dil * (dy * Wp - 1), &full_bar[st]);
+          const int y0 = p0 + a.dil * (dy * Wp - 1);
+          if (TP == 1) {
+            mbar_expect_tx(&full_bar[st], (uint32_t)a.slab_rows * C * 2);
+            tma_2d(s_a + st * kSlabStride, &tm_act, 0, y0, &full_bar[st]);
+          } else {
+            mbar_expect_tx(&full_bar[st], (uint32_t)(FS::kBoxes * kBoxRows * C * 2));
+            for (int b = 0; b < FS::kBoxes; ++b)
+              tma_2d(s_a + st * kSlabStride + b * kBoxRows * C * 2, &tm_act, 0, y0 + b * kBoxRows, &full_bar[st]);
+          }
         }
       }
     }
@@ -244,7 +279,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t d = tmem + acc * C;
+        const uint32_t d = tmem + acc * (C * TP);
         for (int r = 0; r < 3; ++r, ++it) {
           const uint32_t st = it % kStages, ph = (it / kStages) & 1u;
           if (!mbar_wait(&full_bar[st], ph, &s_abort)) {
@@ -260,7 +295,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t sa = slab + 128 * c * a.dil, sb = smem_u32(s_w + (3 * r + c) * kTapBytes);
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-              tc_mma(d, sdesc(sa + 32 * k, 16, 1024), sdesc(sb + 32 * k, 16, 1024), idesc, (r | c | k) ? 1u : 0u);
+#pragma unroll
+              for (int h = 0; h < TP; ++h)  // the TP tiles' MMAs interleaved: independent accumulators
+                tc_mma(d + C * h, sdesc(sa + BM * 128 * h + 32 * k, 16, 1024), sdesc(sb + 32 * k, 16, 1024), idesc,
+                       (r | c | k) ? 1u : 0u);
           }
           tc_commit(&empty_bar[st]);
         }
@@ -283,62 +321,78 @@ __global__ void __launch_bounds__(kThreads, 1)
         break;
       }
       tc_fence_after();
-      float v[64];
-      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + acc * C;
-      tmem_ld16(base + 0, *reinterpret_cast<float(*)[16]>(&v[0]));
-      tmem_ld16(base + 16, *reinterpret_cast<float(*)[16]>(&v[16]));
-      tmem_ld16(base + 32, *reinterpret_cast<float(*)[16]>(&v[32]));
-      tmem_ld16(base + 48, *reinterpret_cast<float(*)[16]>(&v[48]));
+      __syncwarp();  // tcgen05.ld is warp-wide: lanes that left the last pixel early meet here
+      // the whole buffer (TP accumulators) into registers, then it is released to the MMA warp
+      float vv[TP][64];
+      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + acc * (C * TP);
+#pragma unroll
+      for (int hh = 0; hh < TP; ++hh)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) tmem_ld16(base + C * hh + 16 * j, *reinterpret_cast<float(*)[16]>(&vv[hh][16 * j]));
       tmem_wait_ld();
       tc_fence_before();
       mbar_arrive(&acc_empty[acc]);
-      const int p = tile * BM + row;
-      if (p >= a.n_pix) continue;
-      const int xx = p % Wp, yy = (p / Wp) % a.Hp;
-      const bool interior = xx >= kPad && xx < Wp - kPad && yy >= kPad && yy < a.Hp - kPad;
-      if (EPI == EPI_HEAD) {
-        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (interior) o = make_float4(v[0] + s_bias[0], v[1] + s_bias[1], v[2] + s_bias[2], v[3] + s_bias[3]);
-        reinterpret_cast<float4*>(a.out)[p] = o;
-        continue;
-      }
-      uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(a.out) + (size_t)p * C);
-      if (!interior) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) dst[j] = make_uint4(0, 0, 0, 0);
-        continue;
-      }
-      const uint4* rsrc = (EPI == EPI_BIAS_RES_RELU || EPI == EPI_RES_MASK)
-                              ? reinterpret_cast<const uint4*>(a.res + (size_t)p * C)
-                              : nullptr;
-      const uint4* msrc = (EPI == EPI_MASK || EPI == EPI_RES_MASK) ? reinterpret_cast<const uint4*>(a.mask + (size_t)p * C)
-                                                                    : nullptr;
+      for (int hh = 0; hh < TP; ++hh) {
+        const float (&v)[64] = vv[hh];
+        do {  // one pixel; lanes that have nothing to write leave through break
+          const int p = (tile * TP + hh) * BM + row;
+          if (p >= a.n_pix) break;
+          const int xx = p % Wp, yy = (p / Wp) % a.Hp;
+          const bool interior = xx >= kPad && xx < Wp - kPad && yy >= kPad && yy < a.Hp - kPad;
+          if (EPI == EPI_HEAD) {
+            float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (interior) o = make_float4(v[0] + s_bias[0], v[1] + s_bias[1], v[2] + s_bias[2], v[3] + s_bias[3]);
+            reinterpret_cast<float4*>(a.out)[p] = o;
+            break;
+          }
+          uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(a.out) + (size_t)p * C);
+          if (!interior) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        float x[8];
+            for (int j = 0; j < 8; ++j) dst[j] = make_uint4(0, 0, 0, 0);
+            break;
+          }
+          const uint4* rsrc = (EPI == EPI_BIAS_RES_RELU || EPI == EPI_RES_MASK)
+                                  ? reinterpret_cast<const uint4*>(a.res + (size_t)p * C)
+                                  : nullptr;
+          const uint4* msrc = (EPI == EPI_MASK || EPI == EPI_RES_MASK) ? reinterpret_cast<const uint4*>(a.mask + (size_t)p * C)
+                                                                        : nullptr;
+          // every load of the pixel before its first store: the stores may alias the sources as far
+          // as the compiler knows, so loads left in the loop below would each wait for the one before
+          uint4 rv[8], mv[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) x[i] = v[8 * j + i];
-        if (EPI == EPI_BIAS_RELU || EPI == EPI_BIAS_RES_RELU) {
+          for (int j = 0; j < 8; ++j) {
+            if (rsrc) rv[j] = rsrc[j];
+            if (msrc) mv[j] = msrc[j];
+          }
 #pragma unroll
-          for (int i = 0; i < 8; ++i) x[i] += s_bias[8 * j + i];
-        }
-        if (rsrc) {
-          float r[8];
-          unpack8(rsrc[j], r);
+          for (int j = 0; j < 8; ++j) {
+            float x[8];
 #pragma unroll
-          for (int i = 0; i < 8; ++i) x[i] += r[i];
-        }
-        if (EPI == EPI_BIAS_RELU || EPI == EPI_BIAS_RES_RELU) {
+            for (int i = 0; i < 8; ++i) x[i] = v[8 * j + i];
+            if (EPI == EPI_BIAS_RELU || EPI == EPI_BIAS_RES_RELU) {
 #pragma unroll
-          for (int i = 0; i < 8; ++i) x[i] = fmaxf(x[i], 0.f);
-        }
-        if (msrc) {
-          float m[8];
-          unpack8(msrc[j], m);
+              for (int i = 0; i < 8; ++i) x[i] += s_bias[8 * j + i];
+            }
+            if (rsrc) {
+              float r[8];
+              unpack8(rv[j], r);
 #pragma unroll
-          for (int i = 0; i < 8; ++i) x[i] = m[i] > 0.f ? x[i] : 0.f;
-        }
-        dst[j] = make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7]));
+              for (int i = 0; i < 8; ++i) x[i] += r[i];
+            }
+            if (EPI == EPI_BIAS_RELU || EPI == EPI_BIAS_RES_RELU) {
+#pragma unroll
+              for (int i = 0; i < 8; ++i) x[i] = fmaxf(x[i], 0.f);
+            }
+            if (msrc) {
+              float m[8];
+              unpack8(mv[j], m);
+#pragma unroll
+              for (int i = 0; i < 8; ++i) x[i] = m[i] > 0.f ? x[i] : 0.f;
+            }
+            dst[j] = make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7]));
+          }
+        } while (0);
       }
     }
   }
@@ -346,7 +400,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(FS::kTmemCols) : "memory");
   }
 }
 
@@ -530,7 +584,7 @@ cudaError_t conv3x3(const ConvShape& s, const __nv_bfloat16* in, const __nv_bflo
   const int n_pix = s.N * (s.H + 2 * kPad) * (s.W + 2 * kPad);
   const int slab_rows = BM + 2 * s.dil;
   CUtensorMap tm_a, tm_w;
-  if (encode_act_map(&tm_a, in, n_pix, slab_rows) || encode_act_map(&tm_w, w, 9 * C, C)) return cudaErrorInvalidValue;
+  if (encode_act_map(&tm_w, w, 9 * C, C)) return cudaErrorInvalidValue;
   FwdArgs a;
   a.bias = bias;
   a.res = res;
@@ -541,16 +595,18 @@ cudaError_t conv3x3(const ConvShape& s, const __nv_bfloat16* in, const __nv_bflo
   a.Wp = s.W + 2 * kPad;
   a.dil = s.dil;
   a.slab_rows = slab_rows;
-  a.n_tiles = (n_pix + BM - 1) / BM;
   a.err = err;
-  const int smem = kWBytes + kStages * kSlabStride + 1024;
-  const int grid = std::min(conv_grid(), a.n_tiles);
 #define FIP_SG_LAUNCH(E)                                                                                  \
   case E: {                                                                                                \
+    constexpr int TP = tiles_per_unit<E>();                                                                \
+    if (encode_act_map(&tm_a, in, n_pix, TP == 1 ? slab_rows : kBoxRows)) return cudaErrorInvalidValue;   \
+    a.n_tiles = (n_pix + BM * TP - 1) / (BM * TP); /* work units of TP tiles */                           \
+    const int smem = FwdShape<TP>::kSmem;                                                                  \
+    const int grid = std::min(conv_grid(), a.n_tiles);                                                     \
     static std::atomic<uint64_t> cfg{0};                                                                   \
-    const cudaError_t e = ensure_dynamic_smem(conv3x3_kernel<E>, smem, cfg);                              \
+    const cudaError_t e = ensure_dynamic_smem(conv3x3_kernel<E, TP>, smem, cfg);                          \
     if (e != cudaSuccess) return e;                                                                        \
-    conv3x3_kernel<E><<<grid, kThreads, smem, stream>>>(tm_a, tm_w, a);                                    \
+    conv3x3_kernel<E, TP><<<grid, kThreads, smem, stream>>>(tm_a, tm_w, a);                                \
     break;                                                                                                 \
   }
   switch (epi) {
