@@ -10,12 +10,13 @@ graph with the state resident in HBM (the 1.18 GB working set of a step is far l
 126 MB L2, so no flush is needed); `e2e` runs the same steps through the C ABI with the state
 uploaded from and downloaded to pinned host buffers around every batch of steps. The roofline
 uses 32 algorithmic bytes per cell update (read h, qx, qy, terrain, kSt; write h, qx, qy) and the
-stencil kernel's average launch time, from CUDA events around every stencil launch inside the
-timed graph. With N > 1 (torchrun) every rank runs an independent replica ("replicas only").
+stencil kernel's average launch time, from CUDA events around every stencil launch in a second
+graph of K steps (event nodes between the launches keep them from overlapping, so the headline
+graph has none). With N > 1 (torchrun) every rank runs an independent replica ("replicas only").
 
 --impl reference times the reference's algorithm on the host cores: the reference's path is CUDA
-only, so its CPU stand-in is the FP64 restatement (oracle port) with all host threads, on a
-bounded row band of the same scenario.
+only, so its CPU stand-in is the FP64 restatement (oracle port) of the whole scenario (every
+cell, its boundary conditions and dt control) with all host threads.
 
 Two informational objects ride on the same line (N = 1 only): `ensemble` (64 scenarios of
 W, H ~ U[256, 2048] as one batched ensemble, every tile computed, autotuned tile shape, against

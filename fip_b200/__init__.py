@@ -132,7 +132,8 @@ class Simulation:
         return a.value, b.value
 
     def step_timed(self, n: int):
-        """n steps in one graph, timed on the device: (total ms, stencil ms/launch, post ms/launch)."""
+        """n steps in one graph, timed on the device: total ms; then n more steps with an event
+        around every launch: stencil and post ms per launch. Returns the three."""
         t, a, b = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         _lib.check(_lib.lib().fip_step_timed(self._h, int(n), ctypes.byref(t), ctypes.byref(a), ctypes.byref(b)))
         return t.value, a.value, b.value

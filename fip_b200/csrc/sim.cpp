@@ -1078,41 +1078,54 @@ int fip_step_timed(fip_handle* h, int n, float* total_ms, float* stencil_ms, flo
     h->h_ctl->next_sample = kInf;
     h->h_ctl->next_save = kInf;
     h->h_ctl->target = kInf;
-    h->h_ctl->steps_left = n;
+    const bool per_launch = stencil_ms || post_ms;
+    h->h_ctl->steps_left = per_launch ? 2 * n : n;
     h->h_ctl->stop = 0;
     h->h_ctl->stop_reason = 0;
     h->write_ctl_fields();
-    std::vector<cudaEvent_t> ev(2 * n + 1);
-    for (auto& e : ev) ck(cudaEventCreate(&e), "event");
-    cudaGraph_t g;  // event record nodes (cudaEventRecordExternal) timestamp every launch
-    ck(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "capture");
-    for (int i = 0; i < n; ++i) {
-      ck(cudaEventRecordWithFlags(ev[2 * i], h->stream, cudaEventRecordExternal), "event");
-      ck(fip::launch_rmg_step(h->st, h->grid_ctas, h->stream), "rmg_step");
-      ck(cudaEventRecordWithFlags(ev[2 * i + 1], h->stream, cudaEventRecordExternal), "event");
-      h->launch_post(FIP_POST_MODE_STEP);
-    }
-    ck(cudaEventRecordWithFlags(ev[2 * n], h->stream, cudaEventRecordExternal), "event");
-    ck(cudaStreamEndCapture(h->stream, &g), "capture");
-    cudaGraphExec_t ex;
-    ck(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate");
-    cudaGraphDestroy(g);
-    ck(cudaGraphUpload(ex, h->stream), "cudaGraphUpload");
-    ck(cudaStreamSynchronize(h->stream), "sync");
-    ck(cudaGraphLaunch(ex, h->stream), "cudaGraphLaunch");
-    h->read_ctl();
+    // One graph of n steps; with `events`, event record nodes (cudaEventRecordExternal) timestamp
+    // every launch, which also keeps each launch from overlapping the one before it.
+    auto timed = [&](bool events, std::vector<cudaEvent_t>& ev) {
+      ev.resize(events ? 2 * n + 1 : 2);
+      for (auto& e : ev) ck(cudaEventCreate(&e), "event");
+      cudaGraph_t g;
+      ck(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "capture");
+      ck(cudaEventRecordWithFlags(ev[0], h->stream, cudaEventRecordExternal), "event");
+      for (int i = 0; i < n; ++i) {
+        ck(fip::launch_rmg_step(h->st, h->grid_ctas, h->stream), "rmg_step");
+        if (events) ck(cudaEventRecordWithFlags(ev[2 * i + 1], h->stream, cudaEventRecordExternal), "event");
+        h->launch_post(FIP_POST_MODE_STEP);
+        if (events) ck(cudaEventRecordWithFlags(ev[2 * i + 2], h->stream, cudaEventRecordExternal), "event");
+      }
+      if (!events) ck(cudaEventRecordWithFlags(ev[1], h->stream, cudaEventRecordExternal), "event");
+      ck(cudaStreamEndCapture(h->stream, &g), "capture");
+      cudaGraphExec_t ex;
+      ck(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate");
+      cudaGraphDestroy(g);
+      ck(cudaGraphUpload(ex, h->stream), "cudaGraphUpload");
+      ck(cudaStreamSynchronize(h->stream), "sync");
+      ck(cudaGraphLaunch(ex, h->stream), "cudaGraphLaunch");
+      ck(cudaStreamSynchronize(h->stream), "sync");
+      cudaGraphExecDestroy(ex);
+    };
+    std::vector<cudaEvent_t> ev_total, ev_each;
     double tot = 0, s = 0, p = 0;
     float x = 0;
-    ck(cudaEventElapsedTime(&x, ev[0], ev[2 * n]), "event");
+    timed(false, ev_total);  // the steps as the step loop runs them
+    ck(cudaEventElapsedTime(&x, ev_total[0], ev_total[1]), "event");
     tot = x;
-    for (int i = 0; i < n; ++i) {
-      ck(cudaEventElapsedTime(&x, ev[2 * i], ev[2 * i + 1]), "event");
-      s += x;
-      ck(cudaEventElapsedTime(&x, ev[2 * i + 1], ev[2 * i + 2]), "event");
-      p += x;
+    if (per_launch) {
+      timed(true, ev_each);
+      for (int i = 0; i < n; ++i) {
+        ck(cudaEventElapsedTime(&x, ev_each[2 * i], ev_each[2 * i + 1]), "event");
+        s += x;
+        ck(cudaEventElapsedTime(&x, ev_each[2 * i + 1], ev_each[2 * i + 2]), "event");
+        p += x;
+      }
     }
-    cudaGraphExecDestroy(ex);
-    for (auto& e : ev) cudaEventDestroy(e);
+    h->read_ctl();
+    for (auto& e : ev_total) cudaEventDestroy(e);
+    for (auto& e : ev_each) cudaEventDestroy(e);
     if (total_ms) *total_ms = (float)tot;
     if (stencil_ms) *stencil_ms = (float)(s / n);
     if (post_ms) *post_ms = (float)(p / n);

@@ -139,10 +139,13 @@ int fip_info(fip_handle* h, fip_info_t* out);
  * n_steps eager (not graph) steps: average ms per launch. No counterpart in the reference. */
 int fip_profile_steps(fip_handle* h, int n_steps, float* stencil_ms, float* post_ms);
 
-/* n_steps steps as one CUDA graph with an event record around every stencil launch, timed on
- * the handle's stream: total device ms of the n steps and the average ms per launch of the
- * stencil and post kernels. Sampling, dumps and the target duration are not checked during
- * these steps (the state advances normally otherwise). No counterpart in the reference. */
+/* n_steps steps as one CUDA graph, as the step loop runs them, timed with events on the
+ * handle's stream: total device ms of the n steps. When stencil_ms or post_ms is given, n_steps
+ * more steps run as a second graph with an event record around every launch (which keeps each
+ * launch from overlapping the one before it): the average ms per launch of the stencil and of
+ * the post kernel (the gap between launches included). Sampling, dumps and the target duration
+ * are not checked during these steps (the state advances normally otherwise). No counterpart
+ * in the reference. */
 int fip_step_timed(fip_handle* h, int n_steps, float* total_ms, float* stencil_ms, float* post_ms);
 
 /* Exact-resume checkpoint (replaces the reference's restart through save_state dumps fed back as
