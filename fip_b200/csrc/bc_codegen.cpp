@@ -73,10 +73,12 @@ __device__ float fip_sum_depths(const float* sohle, long long base, long long in
   return __fmul_rn(acc, dx);
 }
 
-// Active tiles of the next step: a tile is computed when a tile of its 3x3 neighbourhood had a
-// nonzero cell after this step (the stencil reaches 2 cells, less than a tile), when it had one
-// after the previous step (its cells in the output buffer are then not yet equal to the input),
-// or when it is sticky. The flags of the previous step are cleared for reuse.
+// Active tiles of the next step: a tile is computed when a cell within 2 of it (the stencil's
+// reach) may have been nonzero after this step -- a cell of the tile itself or of the tiles above
+// and below it, or of the facing edge band (FIP_NZ_EAST / FIP_NZ_WEST) of the three tiles beside
+// it in each neighbouring strip --, when it had a nonzero cell after the previous step (its cells
+// in the output buffer are then not yet equal to the input), or when it is sticky. The flags of
+// the previous step are cleared for reuse.
 __device__ void fip_plan(const FipPostArgs& a, const FipCtl* ctl, int k, int chunk) {
   __shared__ int s_act[FIP_POST_THREADS / 32];
   __shared__ int s_inact[FIP_POST_THREADS / 32];
@@ -91,10 +93,11 @@ __device__ void fip_plan(const FipPostArgs& a, const FipCtl* ctl, int k, int chu
     for (int ds = -1; ds <= 1 && !act; ++ds) {
       const int s2 = sx + ds;
       if (s2 < 0 || s2 >= a.n_sx) continue;
+      const unsigned char need = ds < 0 ? FIP_NZ_EAST : ds > 0 ? FIP_NZ_WEST : FIP_NZ_ANY;
       for (int dy = -1; dy <= 1; ++dy) {
         const int y2 = ty + dy;
         if (y2 < 0 || y2 >= a.n_ty) continue;
-        if (nzc[s2 * a.n_ty + y2]) { act = true; break; }
+        if (nzc[s2 * a.n_ty + y2] & need) { act = true; break; }
       }
     }
     nzp[t] = 0;
@@ -224,13 +227,14 @@ __device__ void fip_ens_plan(const FipEnsPostArgs& a, const FipCtl* ctl, int k, 
     const int local = t - M.tile_base;
     const int sx = local / M.n_ty, ty = local - sx * M.n_ty;
     act = a.sticky[t] || nzp[t] || ctl->force_all;
-    for (int ds = -1; ds <= 1 && !act; ++ds) {
+    for (int ds = -1; ds <= 1 && !act; ++ds) {  // the rule of fip_plan, within the member
       const int s2 = sx + ds;
       if (s2 < 0 || s2 >= M.n_sx) continue;
+      const unsigned char need = ds < 0 ? FIP_NZ_EAST : ds > 0 ? FIP_NZ_WEST : FIP_NZ_ANY;
       for (int dy = -1; dy <= 1; ++dy) {
         const int y2 = ty + dy;
         if (y2 < 0 || y2 >= M.n_ty) continue;
-        if (nzc[M.tile_base + s2 * M.n_ty + y2]) { act = true; break; }
+        if (nzc[M.tile_base + s2 * M.n_ty + y2] & need) { act = true; break; }
       }
     }
     act = act && runs;

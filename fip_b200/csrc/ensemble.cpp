@@ -238,7 +238,7 @@ void fip_ensemble::init(const std::vector<std::string>& paths, const fip_options
   if (max_chunks > 256) throw std::invalid_argument("ensemble too large: more than 131072 tiles of 240 x 16 cells");
   eck(cudaMalloc((void**)&st.sticky, max_tiles), "cudaMalloc");
   for (int b = 0; b < 2; ++b) {
-    eck(cudaMalloc((void**)&st.nz[b], max_tiles), "cudaMalloc");
+    eck(cudaMalloc((void**)&st.nz[b], ((size_t)max_tiles + 3) & ~(size_t)3), "cudaMalloc");
     eck(cudaMalloc((void**)&st.list[b], sizeof(int) * (size_t)max_chunks * FIP_PLAN_CHUNK), "cudaMalloc");
     eck(cudaMalloc((void**)&st.chunk_cnt[b], sizeof(int) * max_chunks), "cudaMalloc");
     eck(cudaMemset(st.chunk_cnt[b], 0, sizeof(int) * max_chunks), "cudaMemset");

@@ -20,6 +20,13 @@
 #define FIP_PLAN_CHUNK 512     // tiles planned per post-kernel block / list chunk
 #define FIP_POST_THREADS 512
 
+// per-tile flags of a state (one byte per tile): some cell of the tile is nonzero; some cell of
+// its first / last few columns is (2 or 4: the stencil reaches 2 cells, so only the first and
+// last two columns feed the tiles of the neighbouring strips)
+#define FIP_NZ_ANY 1
+#define FIP_NZ_WEST 2
+#define FIP_NZ_EAST 4
+
 // stop reasons (bit mask)
 #define FIP_STOP_BUDGET 1      // the requested number of steps ran
 #define FIP_STOP_SAMPLE 2      // duration >= sampling timer: sample before the next step

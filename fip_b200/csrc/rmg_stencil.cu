@@ -53,6 +53,7 @@ constexpr int kNSlotKvarNarrow = 7;
 constexpr int kNSlotUniformNarrow = 8;
 constexpr int kMaxChunks = 256;
 constexpr unsigned long long kWaitNs = 2000000000ull;
+constexpr int kNzBand = 4;  // edge-band width of the tile flags a state's scan sets (>= 2, the stencil's reach)
 
 enum { F_H = 0, F_QX = 1, F_QY = 2, F_S = 3, F_K = 4 };
 
@@ -199,6 +200,14 @@ __device__ __forceinline__ void vfma(float (&d)[N], float2 a, const float (&b)[N
 }
 
 __device__ __forceinline__ bool store_row_flag(int r, int ra) { return r >= ra; }
+
+// OR `bits` into the tile flag byte at p: an atomic OR on the aligned 32-bit word that holds it
+// (flag arrays are allocated in whole words), so that warps setting different bits of one tile
+// do not overwrite each other
+__device__ __forceinline__ void tile_flag_or(unsigned char* p, unsigned bits) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  atomicOr(reinterpret_cast<unsigned*>(a & ~static_cast<uintptr_t>(3)), bits << (8u * static_cast<unsigned>(a & 3)));
+}
 
 // max(a, b, c) as the reference nests it (max(max(DH, h_i), h_east))
 __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
@@ -910,15 +919,24 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
         if (store_row && ((r + 1) % TR == 0 || r + 1 == rb)) {
           // halo lanes hold the neighbouring strips' cells; columns beyond W (zero-filled loads)
           // can only set flags, never clear them
-          if (__any_sync(0xffffffffu, out_lane && nzacc != 0u) && lane == 0) {
-            const int tb = ENS ? lds_at_use(&s_msc[warp][2]) : 0, nt = ENS ? lds_at_use(&s_msc[warp][3]) : nty;
-            nzs[tb + s * nt + r / TR] = 1;
+          if (__any_sync(0xffffffffu, out_lane && nzacc != 0u)) {
+            // edge bands: lane 1 of warp 0 holds the tile's first NC columns, lane 30 of warp
+            // KW - 1 its last NC (at least the two the stencil reaches); one warp sets each band
+            // bit, every warp with a nonzero cell the ANY bit (the conditions are warp-uniform)
+            unsigned f = FIP_NZ_ANY;
+            if (warp == 0 && __shfl_sync(0xffffffffu, nzacc, 1) != 0u) f |= FIP_NZ_WEST;
+            if (warp == KW - 1 && __shfl_sync(0xffffffffu, nzacc, 30) != 0u) f |= FIP_NZ_EAST;
+            if (lane == 0) {
+              const int tb = ENS ? lds_at_use(&s_msc[warp][2]) : 0, nt = ENS ? lds_at_use(&s_msc[warp][3]) : nty;
+              tile_flag_or(nzs + tb + s * nt + r / TR, f);
+            }
           }
           nzacc = 0u;
         }
       }
 
-      nzacc = store_row_flag(r, ra) ? nzacc : 0u;  // the extra row below a run is no part of a tile
+      // the extra row below a run is no part of a tile
+      nzacc = store_row_flag(r, ra) ? nzacc : 0u;
       release_slot(iS);
       // next row: slots advance by one
       iS = i0;
@@ -1004,7 +1022,10 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
 //    those, and the conditions' own cells are covered next;
 //  * it meets a rectangle of `force`: the cells a boundary condition writes, widened by the
 //    stencil's reach (or, with force.all_band, any tile within 4 cells of the edge).
-// Elsewhere a tile whose 3 x 3 neighbourhood is all zero computes zeros, which the plan exploits.
+// Elsewhere a tile computes zeros where its cells and the cells within 2 of it are all zero,
+// which the plan exploits with the flags of each tile (any cell nonzero; any of its first / last
+// kNzBand columns nonzero: the stencil sets those from the columns of the first / last thread of
+// the tile, 4 or 2, at least the 2 it reaches).
 __global__ void init_tiles_kernel(const float* h, const float* qx, const float* qy, const float* sohle, int W, int H,
                                   int pitch, float no_value, int n_ty, int n_tiles, int tile_cols, int tile_rows,
                                   const TileForce force, unsigned char* or_into, unsigned char* sticky,
@@ -1024,17 +1045,22 @@ __global__ void init_tiles_kernel(const float* h, const float* qx, const float* 
       }
     }
     nz = __syncthreads_or(nz);
-    if (threadIdx.x == 0 && nz) or_into[t] = 1;
+    if (threadIdx.x == 0 && nz) or_into[t] |= FIP_NZ_ANY;
     return;
   }
   // the tile widened by the stencil's reach of 2 cells, clipped to the grid
   const int x0 = max(c0 - 2, 0), x1 = min(c1 + 2, W), y0 = max(r0 - 2, 0), y1 = min(r1 + 2, H);
   const int ww = x1 - x0;
+  int nzw = 0, nze = 0;  // nonzero cells in the tile's first / last kNzBand columns
   for (int e = threadIdx.x; e < ww * (y1 - y0); e += blockDim.x) {
     const int r = y0 + e / ww, c = x0 + e % ww;
     const size_t o = (size_t)r * pitch + c;
     const bool nzc = (h[o] != 0.f) || (qx[o] != 0.f) || (qy[o] != 0.f);
-    if (r >= r0 && r < r1 && c >= c0 && c < c1) nz |= nzc;
+    if (r >= r0 && r < r1 && c >= c0 && c < c1) {
+      nz |= nzc;
+      if (c < c0 + kNzBand) nzw |= nzc;
+      if (c >= c1 - kNzBand) nze |= nzc;
+    }
     const bool unwritten = r <= 1 || r >= H - 2 || c <= 1 || c >= W - 2 || sohle[o] == no_value;
     if (nzc && unwritten) st = 1;
   }
@@ -1049,11 +1075,14 @@ __global__ void init_tiles_kernel(const float* h, const float* qx, const float* 
     }
   }
   nz = __syncthreads_or(nz);
+  nzw = __syncthreads_or(nzw);
+  nze = __syncthreads_or(nze);
   st = __syncthreads_or(st);
   if (threadIdx.x == 0) {
+    const unsigned char f = (unsigned char)((nz ? FIP_NZ_ANY : 0) | (nzw ? FIP_NZ_WEST : 0) | (nze ? FIP_NZ_EAST : 0));
     sticky[t] = (unsigned char)st;
-    nz0[t] = (unsigned char)nz;
-    nz1[t] = (unsigned char)nz;
+    nz0[t] = f;
+    nz1[t] = f;
   }
 }
 

@@ -222,7 +222,7 @@ void fip_handle::init(const std::string& yaml, const fip_options& o) {
   fip::bc_tile_force(cfg, &st.force);
   ck(cudaMalloc((void**)&st.sticky, st.n_tiles), "cudaMalloc");
   for (int b = 0; b < 2; ++b) {
-    ck(cudaMalloc((void**)&st.nz[b], st.n_tiles), "cudaMalloc");
+    ck(cudaMalloc((void**)&st.nz[b], ((size_t)st.n_tiles + 3) & ~(size_t)3), "cudaMalloc");
     ck(cudaMalloc((void**)&st.list[b], sizeof(int) * st.n_chunks * FIP_PLAN_CHUNK), "cudaMalloc");
     ck(cudaMalloc((void**)&st.chunk_cnt[b], sizeof(int) * st.n_chunks), "cudaMalloc");
     ck(cudaMemset(st.chunk_cnt[b], 0, sizeof(int) * st.n_chunks), "cudaMemset");

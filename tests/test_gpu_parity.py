@@ -232,6 +232,82 @@ def test_dry_tile_skipping_is_exact(tmp_path):
             assert np.array_equal(ref[k].view(np.uint32), fields[k].view(np.uint32)), k
 
 
+def _band_plan_count(cur, prev, tc, tr, band=4):
+    """Tiles the plan computes for the next step, for states with no sticky tile: a tile that
+    had a nonzero cell in the previous state, or whose own strip has one in it or in the tiles
+    above and below it in the current state, or whose neighbouring strips have one in their
+    facing `band` columns (of the three tiles beside it). Also returns the count of the rule
+    "any nonzero cell in the 3 x 3 tile neighbourhood" for the same states. cur / prev: (h, qx, qy)."""
+    nz = (cur[0] != 0) | (cur[1] != 0) | (cur[2] != 0)
+    nzp = (prev[0] != 0) | (prev[1] != 0) | (prev[2] != 0)
+    H, W = nz.shape
+    n_sx, n_ty = -(-W // tc), -(-H // tr)
+    anyf = np.zeros((n_sx, n_ty), bool)
+    west = np.zeros((n_sx, n_ty), bool)
+    east = np.zeros((n_sx, n_ty), bool)
+    anyp = np.zeros((n_sx, n_ty), bool)
+    for s in range(n_sx):
+        c0, c1 = s * tc, min((s + 1) * tc, W)
+        for t in range(n_ty):
+            blk = nz[t * tr:(t + 1) * tr, c0:c1]
+            anyf[s, t], west[s, t], east[s, t] = blk.any(), blk[:, :band].any(), blk[:, -band:].any()
+            anyp[s, t] = nzp[t * tr:(t + 1) * tr, c0:c1].any()
+    act = n3 = 0
+    for s in range(n_sx):
+        for t in range(n_ty):
+            rows = slice(max(t - 1, 0), t + 2)
+            own = anyp[s, t] or anyf[s, rows].any()
+            side = (s > 0 and east[s - 1, rows].any()) or (s + 1 < n_sx and west[s + 1, rows].any())
+            act += bool(own or side)
+            n3 += bool(anyp[s, t] or anyf[max(s - 1, 0):s + 2, rows].any())
+    return act, n3
+
+
+def test_dry_tile_skipping_across_strip_edges(tmp_path):
+    """Water short of the edge bands of a strip on either side (the first and last thread's four
+    columns of a 480-column tile, which hold the two columns the stencil reaches), and a pond
+    across a strip edge: the strip beside a pond is planned only once water reaches its facing
+    band. The plan of the second step has exactly the tiles that rule names (fewer than "any
+    nonzero cell in the 3 x 3 tile neighbourhood" would), and runs with dry-tile skipping stay
+    bit-identical to every-tile runs while the fronts cross the strip edges."""
+    from fip_b200 import synth
+
+    W, H = 1500, 192
+    y = np.arange(H, dtype=np.float32)[:, None]
+    x = np.arange(W, dtype=np.float32)[None, :]
+    terr = (0.05 * np.sin(x / 29.0) * np.cos(y / 17.0)).astype(np.float32)
+    depth = np.zeros((H, W), np.float32)
+    depth[40:80, 466:474] = 1.0      # after one step still west of strip 0's east band (476-479)
+    depth[100:140, 966:980] = 0.9    # after one step still east of strip 2's west band (960-963)
+    depth[150:170, 478:490] = 0.7    # across the edge of strips 0 and 1
+    files = {}
+    for k, a in (("terrain", terr), ("z", terr + depth)):
+        files[k] = str(tmp_path / f"e_{k}.bin")
+        synth.write_grid(files[k], a)
+    cfg = {"name": str(tmp_path / "e"), "terrain": [files["terrain"], 0], "z": [files["z"], 0], "W": W, "H": H,
+           "dx": 2.0, "dt": 0.05, "duration": 1000, "kSt": 30, "variable_dt": False}
+    path = str(tmp_path / "e.yml")
+    synth.write_yaml(path, cfg)
+    res = []
+    for all_tiles, graphs in ((True, False), (False, True), (False, False)):
+        sim = _sim(path, quiet=True, all_tiles=all_tiles, use_graphs=graphs)
+        sim.step(1)
+        st = {k: sim.field(k) for k, _ in FIELDS}
+        planned = sim.info().active_tiles  # plan of step 2
+        sim.step(239)
+        res.append(({k: sim.field(k) for k, _ in FIELDS}, st, planned, sim.info().n_tiles))
+        sim.close()
+    ref = res[0][0]
+    # both fronts crossed into strip 1
+    assert float(np.abs(ref["h"][40:80, 480:482]).max()) > 0 and float(np.abs(ref["h"][100:140, 958:960]).max()) > 0
+    for fields, st, planned, n in res[1:]:
+        want, n3 = _band_plan_count((st["h"], st["qx"], st["qy"]), (st["h_prev"], st["qx_prev"], st["qy_prev"]),
+                                    480, 32)
+        assert planned == want < n3 <= n, (planned, want, n3, n)
+        for k, _ in FIELDS:
+            assert np.array_equal(ref[k].view(np.uint32), fields[k].view(np.uint32)), k
+
+
 def test_variable_dt_matches_oracle(tmp_path):
     y = random_case(tmp_path, 120, 96, seed=11, dt=0.05, variable_dt=True)
     sim = _sim(y, quiet=True)
