@@ -15,8 +15,9 @@
 //     neighbours with warp shuffles and do the arithmetic on FP32x2 pairs of columns;
 //   * work = the concatenation of the active tiles' rows (strip-major), split evenly over the
 //     persistent CTAs, so vertically adjacent active tiles are marched without re-staging;
-//   * each CTA folds its CFL minimum into ctl->cfl_bits with one atomicMin per warp, marks the
-//     tiles whose new state has a nonzero cell, and (every hmax_every iterations) folds hmax.
+//   * each CTA folds its CFL minimum into ctl->cfl_bits with one atomicMin per warp, flags the
+//     tiles whose new state has a nonzero cell (and whether one lies in the tile's first or last
+//     columns: FIP_NZ_*), and (every hmax_every iterations) folds hmax.
 // Every wait on an mbarrier is bounded (2 s of %globaltimer); on expiry the kernel records
 // FIP_DEVERR_* in ctl->error and returns after draining its own copies.
 #include <cuda.h>
@@ -1012,9 +1013,9 @@ __global__ void __launch_bounds__((KW + 1) * 32, StepShape<NC, KW>::kMinCtas)
   }
 }
 
-// Per tile of a tile_cols x tile_rows grid: sticky flag and whether buffer (h, qx, qy) has a
-// nonzero cell (into nz0 and nz1). With or_into set, the nonzero flag is OR-ed into or_into[t]
-// instead and nothing else is written.
+// Per tile of a tile_cols x tile_rows grid: sticky flag and the FIP_NZ_* flags of buffer
+// (h, qx, qy) (into nz0 and nz1). With or_into set, FIP_NZ_ANY is OR-ed into or_into[t] where the
+// tile has a nonzero cell instead, and nothing else is written.
 // A tile is sticky (computed every step) when
 //  * a cell the step never writes holds water within 2 cells of it (the step reads 2 cells
 //    around each cell it updates): no_data cells, and the cells within 1 of the edge that the

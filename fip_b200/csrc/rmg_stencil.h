@@ -30,7 +30,7 @@ struct StencilState {
   float* hmax;
   FipCtl* ctl;  // device control block
   unsigned char* sticky;  // per tile: always active (boundary-condition cells, static water on cells the step never writes)
-  unsigned char* nz[2];   // per tile: some cell of the new state is nonzero, by iteration parity
+  unsigned char* nz[2];   // per tile: FIP_NZ_* flags of the new state, by iteration parity (whole words)
   int* list[2];           // active tiles by chunk (front) / inactive tiles (back), by parity
   int* chunk_cnt[2];      // active tiles per chunk, by parity
   int W, H, pitch;
@@ -60,7 +60,7 @@ int make_tensor_maps(StencilState* st);
 // One rmg step over the active tiles of the current plan (reads ctl on the device).
 cudaError_t launch_rmg_step(const StencilState& st, int grid_ctas, cudaStream_t stream);
 
-// Per-tile sticky flags and the nonzero flags of state buffer `parity` (into both nz slots).
+// Per-tile sticky flags and the FIP_NZ_* flags of state buffer `parity` (into both nz slots).
 cudaError_t launch_init_tiles(const StencilState& st, int parity, cudaStream_t stream);
 
 // The same for one region of a packed ensemble (pointers at the member's first row, flags at its
