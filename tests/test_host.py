@@ -48,6 +48,47 @@ def test_validate_and_parse(tmp_path):
         validate(str(bad))
 
 
+def test_validation_messages_follow_the_reference(tmp_path):
+    """Every check of validateSimDataConfig (src/simdata.cpp:152-236), reported on stderr as the
+    reference reports it (1-based line of the offending node, the root map for missing keys),
+    all of them before the load fails."""
+    import subprocess
+    import sys
+
+    y = tmp_path / "v.yml"
+    y.write_text("name: x\n"                           # 1
+                 "terrain: [t.bin]\n"                  # 2: path without its byte offset
+                 "W: 8\n"                              # 3  (H missing)
+                 "dt: 0.1\n"
+                 "dx: 2\n"
+                 "duration: 10\n"
+                 "kSt: 30\n"
+                 "kSt_var: [k.bin, 0]\n"               # 8: both kSt_var and kSt
+                 "boundary_conditions:\n"
+                 "  - side: left\n"                    # 10: q without its q value
+                 "    type: q\n"
+                 "    z: [a.csv, 0]\n"                 # 12: series without its data column
+                 "  - type: z\n"                       # 13: side and z missing
+                 "sampling_interval: 5\n")             # no sampling points
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from fip_b200 import validate, FipError\n"
+            "try:\n    validate(%r)\nexcept FipError as e:\n    print(e.code)\n") % (ROOT, str(y))
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert p.stdout.strip() == str(_lib.FIP_ERR_CONFIG), (p.stdout, p.stderr)
+    got = [ln for ln in p.stderr.splitlines() if ln.strip()]
+    assert got == [
+        'Config error at line 1: "H" missing',
+        'Config error at line 8: Both "kSt_var" and "kSt" defined',
+        'Config error at line 2: file path "terrain" needs format [path, byte_offset]',
+        'Config error at line 10: "q" missing',
+        'Config error at line 12: timeseries "z" needs format [csv_filename, int_time_column, int_data_column]',
+        'Config error at line 13: "side" missing',
+        'Config error at line 13: "z" missing',
+        "Configuration error: sampling interval specified but no sampling points given",
+        "Warning: no save_state times given",
+    ], got
+
+
 def test_defaults_follow_the_reference(tmp_path):
     """variable_dt defaults to true, kSt to 30, no_data to -9999 (src/simdata.cpp:245-254)."""
     terr = np.zeros((8, 8), np.float32)
