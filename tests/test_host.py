@@ -89,6 +89,31 @@ def test_validation_messages_follow_the_reference(tmp_path):
     ], got
 
 
+def test_documented_parameter_forms(tmp_path):
+    """Every form of the reference's parameter table (README.md:46-64): [path, byte offset]
+    grids, a duration and save_state times as products, block and flow-style sampling points, a
+    time-series condition over the whole side and a closed range of another side."""
+    synth.write_grid(str(tmp_path / "t.bin"), np.zeros((12, 10), np.float32), offset=36)
+    (tmp_path / "s.csv").write_text("t;z\n0;1.5\n3600;2.5\n")
+    y = tmp_path / "p.yml"
+    y.write_text(f"name: p\nterrain: [{tmp_path}/t.bin, 36]\nW: 10\nH: 12\ndx: 3\ndt: 0.1\n"
+                 "duration: 3600*24*12\nkSt: 30.0\nvariable_dt: true\nno_data: -1\n"
+                 "save_state:\n  - 3600 * 24 * 0.5\n  - 3600 * 24 * 2.5\n"
+                 "sampling:\n  - x: 0\n    y: 7\n    label: sample1\n    type: z\n"
+                 "  - { x: 4, y: 7, label: sample2, type: qx }\n"
+                 "sampling_interval: 100\n"
+                 f"boundary_conditions:\n  - side: left\n    type: z\n    z: [{tmp_path}/s.csv, 0, 1]\n"
+                 "  - side: right\n    type: close\n    from: 0\n    to: 5\n")
+    c = config_json(str(y))
+    assert c["target_duration"] == 3600 * 24 * 12 and c["save_state"] == [43200, 216000]
+    assert c["sampling"] == [{"x": 0, "y": 7, "label": "sample1", "type": "z"},
+                             {"x": 4, "y": 7, "label": "sample2", "type": "qx"}]
+    assert c["sampling_interval"] == 100 and c["variable_dt"] is True and c["no_data"] == -1 and c["kSt"] == 30
+    bcs = [(b["side"], b["type"], b["from"], b["to"]) for b in c["boundary_conditions"]]
+    assert bcs == [("left", "z", 0, 11), ("right", "close", 0, 5)]
+    assert c["boundary_conditions"][0]["series"] and c["boundary_conditions"][0]["z_v"] == [1.5, 2.5]
+
+
 def test_defaults_follow_the_reference(tmp_path):
     """variable_dt defaults to true, kSt to 30, no_data to -9999 (src/simdata.cpp:245-254)."""
     terr = np.zeros((8, 8), np.float32)
